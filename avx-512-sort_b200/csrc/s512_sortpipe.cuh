@@ -1,0 +1,761 @@
+// s512_sortpipe.cuh -- partition-then-sort pipeline for one GPU.
+//
+// The reference sorts by recursive two-way partitioning (Partition512,
+// sort512.hpp:5729-5912, driven by CoreSort 5947-5958 with the pseudo-median
+// pivot of CoreSortGetPivot 5916-5927) down to leaves of at most 16 vectors
+// (SortLimite = 16*64/sizeof(T), 5949), which SmallSort16V sorts with bitonic
+// networks.  This file keeps that method and widens each step for a GPU:
+//
+//   * a pivot becomes up to 255 splitters drawn from a random sample of the
+//     segment (sorted on the device), so one partition pass splits a segment
+//     into up to 256 buckets instead of 2;
+//   * splitter values that repeat in the sample get an equality bucket (keys
+//     equal to that value need no further sorting), which removes the
+//     reference's quadratic behaviour on few-distinct and sorted inputs;
+//   * the partition pass is out of place and "one sweep": every tile of keys
+//     computes its bucket histogram, publishes it, and learns the number of
+//     keys of each bucket in all earlier tiles from a decoupled look-back over
+//     per-tile status words, then scatters its keys through shared memory so
+//     global writes are coalesced.  Bucket b of a segment is written into a
+//     region whose capacity comes from the sample (a 6-sigma bound); a bucket
+//     that outgrows it is reported and the level is redone with exact counts;
+//   * buckets at most a leaf's capacity are sorted by the bitonic networks of
+//     s512_bitonic.cuh (one warp or one block per bucket, by size class) and
+//     written to their final place; larger buckets become the segments of the
+//     next partition level.
+#pragma once
+
+#include "s512_bitonic.cuh"
+
+namespace s512 {
+
+constexpr int NB = 256;            // buckets per segment per pass (max)
+constexpr int SAMPLE_N = 16384;    // keys sampled per segment
+constexpr int COPY_CHUNK = 16384;  // equality buckets are copied in chunks of this size
+constexpr unsigned long long ST_INC = 1ull << 63;  // status: inclusive prefix
+constexpr unsigned long long ST_AGG = 1ull << 62;  // status: tile aggregate only
+constexpr unsigned long long ST_VAL = (1ull << 62) - 1;
+
+// A segment to partition at some level.
+struct SegDesc {
+    uint64_t in_off;     // first key in the level's input buffer
+    uint64_t count;      // number of keys
+    uint64_t final_off;  // where the segment's keys end in the final output
+    uint64_t out_base;   // start of the segment's bucket regions in the level's output
+    uint32_t tile_start; // first global tile index of the segment
+    uint32_t ntiles;
+};
+
+// Splitters of one segment and the layout of its bucket regions.
+template <typename K>
+struct SplitSet {
+    K tree[NB];            // Eytzinger tree of the unique splitters, nodes 1..255, padded with max
+    K uniq[NB];            // unique splitters in ascending order (padded with max)
+    uint64_t region_off[NB];  // bucket region start, relative to SegDesc::out_base
+    uint64_t region_cap[NB];  // bucket region capacity (keys)
+    uint8_t range_b[NB];   // bucket of keys with lower_bound index j that are not equal to uniq[j]
+    uint8_t eq_b[NB];      // bucket of keys equal to uniq[j] when splitter j has an equality bucket
+    uint32_t eq_mask[NB / 32];     // splitter j has an equality bucket
+    uint32_t bucket_eq[NB / 32];   // bucket b is an equality bucket
+    uint32_t nbuckets;
+    uint32_t has_eq;
+    uint32_t nuniq;
+    uint32_t pad_;
+};
+
+// A bucket that a leaf kernel sorts (or copies) into its final place.
+template <typename K>
+struct LeafItem {
+    const K* src;        // encoded keys in a level buffer
+    uint64_t dst;        // index of the first key in the caller's output
+    uint32_t count;
+    uint32_t pad_;
+};
+
+// Leaf size classes.  Class 0 is one warp per bucket; the others are one
+// block of THREADS x IPT keys per bucket.  COPY is for equality buckets.
+constexpr int NCLASS = 7;
+constexpr int CLS_COPY = NCLASS;  // index of the copy list
+__host__ __device__ constexpr int class_cap(int key_bytes, int c) {
+    // u32: 256 512 1024 2048 4096 8192 16384 ; u64: 256 512 1024 2048 4096 8192 (8192)
+    return key_bytes == 4 ? (256 << c) : (c >= 5 ? 8192 : (256 << c));
+}
+__host__ __device__ constexpr uint32_t leaf_max(int key_bytes) { return key_bytes == 4 ? 16384u : 8192u; }
+__host__ __device__ inline int class_of(int key_bytes, uint32_t count) {
+    int c = 0;
+    while (c < NCLASS - 1 && (uint32_t)class_cap(key_bytes, c) < count) ++c;
+    return c;
+}
+
+// Number of buckets to aim for in a segment of `count` keys: enough that the
+// average bucket is ~leaf_max/4, at most 256.
+__host__ __device__ inline int target_buckets(int key_bytes, uint64_t count) {
+    uint64_t want = (count * 4 + leaf_max(key_bytes) - 1) / leaf_max(key_bytes);
+    if (want < 2) want = 2;
+    if (want > NB) want = NB;
+    return (int)want;
+}
+
+// Upper bound of the total region capacity the splitter kernel may lay out
+// for a segment of `count` keys (see splitter_kernel): 2.01*count + 4096.
+__host__ __device__ inline uint64_t region_bound(uint64_t count) {
+    return count * 2 + count / 100 + 4096;
+}
+
+// Level control block (device); read back by the host after each level.
+struct LevelCtl {
+    uint32_t tile_counter;
+    uint32_t err;
+    uint32_t n_next;          // segments for the next level
+    uint32_t n_items[NCLASS + 1];
+    uint32_t ntiles_next;
+    uint64_t next_keys;       // keys in next-level segments
+    uint64_t bound_next;      // region bound of the next level
+    uint32_t max_bucket;      // largest bucket seen this level
+    uint32_t nonempty;        // non-empty buckets this level
+    uint64_t level_keys;      // keys partitioned this level
+};
+
+// ===========================================================================
+// 1. Sampling: SAMPLE_N keys per segment at hashed positions (with replacement)
+
+template <typename Codec>
+__global__ void sample_kernel(Codec in, const SegDesc* __restrict__ segs, uint32_t nsegs,
+                              typename Codec::Key* __restrict__ samples, uint64_t seed) {
+    const uint32_t s = blockIdx.x;
+    if (s >= nsegs) return;
+    const SegDesc sd = segs[s];
+    for (int i = threadIdx.x; i < SAMPLE_N; i += blockDim.x) {
+        const uint64_t h = mix64(seed ^ ((uint64_t)s << 32) ^ (uint64_t)i);
+        const uint64_t pos = __umul64hi(h, sd.count);
+        samples[(size_t)s * SAMPLE_N + i] = in.load(sd.in_off + pos);
+    }
+}
+
+// 2. Sorting the samples: one block of 1024 threads x 16 keys per segment.
+template <typename K>
+__global__ void __launch_bounds__(1024) sample_sort_kernel(K* __restrict__ samples, uint32_t nsegs) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* smem = reinterpret_cast<K*>(smem_raw);
+    constexpr int IPT = SAMPLE_N / 1024;
+    K* p = samples + (size_t)blockIdx.x * SAMPLE_N;
+    // coalesced load into shared memory, then the blocked register layout
+    for (int i = threadIdx.x; i < SAMPLE_N; i += 1024) smem[i] = p[i];
+    __syncthreads();
+    K x[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
+    __syncthreads();
+    block_bitonic_sort<K, 1024, IPT>(x, smem);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
+    __syncthreads();
+    for (int i = threadIdx.x; i < SAMPLE_N; i += 1024) p[i] = smem[i];
+}
+
+// 3. Splitters and bucket regions: one block of 256 threads per segment.
+template <typename K>
+__device__ __forceinline__ uint32_t lower_bound_dev(const K* a, uint32_t n, K v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+template <typename K>
+__device__ __forceinline__ uint32_t upper_bound_dev(const K* a, uint32_t n, K v) {
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (!(v < a[mid])) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ samples, const SegDesc* __restrict__ segs,
+                                                       uint32_t nsegs, SplitSet<K>* __restrict__ splits,
+                                                       int key_bytes) {
+    const uint32_t s = blockIdx.x;
+    if (s >= nsegs) return;
+    __shared__ K cand[NB];
+    __shared__ K uniq[NB];
+    __shared__ uint32_t eqf[NB];
+    __shared__ uint32_t wtot[8];
+    __shared__ uint32_t total_u, total_eq;
+    __shared__ uint64_t cap_s[NB];
+    __shared__ uint64_t wtot64[8];
+    __shared__ uint64_t cap_total;
+
+    const K* smp = samples + (size_t)s * SAMPLE_N;
+    const SegDesc sd = segs[s];
+    SplitSet<K>* out = splits + s;
+    const int t = threadIdx.x;
+    const int nb = target_buckets(key_bytes, sd.count);
+    const int ncand = nb - 1;
+
+    // candidate splitters at the sample quantiles
+    K c = KeyMax<K>::value;
+    if (t < ncand) c = smp[(uint32_t)(((uint64_t)(t + 1) * SAMPLE_N) / nb) - 1];
+    cand[t] = c;
+    __syncthreads();
+    const bool valid = t < ncand;
+    const bool first = valid && (t == 0 || cand[t] != cand[t - 1]);
+    const bool dup = valid && ((t > 0 && cand[t] == cand[t - 1]) || (t + 1 < ncand && cand[t] == cand[t + 1]));
+    uint32_t j = block_exclusive_scan_first<NB, uint32_t>(first ? 1u : 0u, wtot, &total_u);
+    if (first) {
+        uniq[j] = c;
+        eqf[j] = dup ? 1u : 0u;
+    }
+    __syncthreads();
+    const uint32_t K_u = total_u;
+    if (t >= (int)K_u) {
+        uniq[t] = KeyMax<K>::value;
+        eqf[t] = 0;
+    }
+    __syncthreads();
+    // bucket ids: range_j, then eq_j if splitter j has one; the last range bucket is K_u
+    const uint32_t my_eq = (t < (int)K_u) ? eqf[t] : 0u;
+    const uint32_t eq_before = block_exclusive_scan_first<NB, uint32_t>(my_eq, wtot, &total_eq);
+    const uint32_t range_id = (uint32_t)t + eq_before;  // valid for t <= K_u
+    if (t <= (int)K_u) out->range_b[t] = (uint8_t)range_id;
+    else out->range_b[t] = 0;
+    out->eq_b[t] = (uint8_t)(my_eq ? range_id + 1 : 0);
+    const uint32_t nbk = K_u + 1 + total_eq;
+
+    // sample counts per bucket -> capacities
+    // range bucket j (t <= K_u): keys in (uniq[j-1], uniq[j]] or (uniq[j-1], uniq[j]) if eq_j
+    uint64_t cap_range = 0, cap_eq = 0;
+    const double scale = (double)sd.count / (double)SAMPLE_N;
+    auto cap_of = [&](uint32_t cnt) -> uint64_t {
+        double v = ((double)cnt + 6.0 * sqrt((double)cnt + 1.0) + 16.0) * scale;
+        uint64_t cap = (uint64_t)ceil(v);
+        if (cap > sd.count) cap = sd.count;
+        return (cap + 15) & ~15ull;
+    };
+    if (t <= (int)K_u) {
+        const uint32_t lo = (t == 0) ? 0u : upper_bound_dev<K>(smp, SAMPLE_N, uniq[t - 1]);
+        uint32_t hi;
+        if (t == (int)K_u) hi = SAMPLE_N;
+        else hi = my_eq ? lower_bound_dev<K>(smp, SAMPLE_N, uniq[t]) : upper_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
+        cap_range = cap_of(hi > lo ? hi - lo : 0u);
+        if (my_eq) {
+            const uint32_t e0 = lower_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
+            const uint32_t e1 = upper_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
+            cap_eq = cap_of(e1 - e0);
+        }
+    }
+    // scatter capacities into bucket order
+    if (t < NB) cap_s[t] = 0;
+    __syncthreads();
+    if (t <= (int)K_u) {
+        cap_s[range_id] = cap_range;
+        if (my_eq) cap_s[range_id + 1] = cap_eq;
+    }
+    __syncthreads();
+    const uint64_t my_cap = cap_s[t];
+    const uint64_t off = block_exclusive_scan_first<NB, uint64_t>(my_cap, wtot64, &cap_total);
+    out->region_off[t] = off;
+    out->region_cap[t] = my_cap;
+    // Eytzinger tree over uniq[0..254]: node i at depth d has in-order index
+    // (2*(i - 2^d) + 1) * 2^(7-d) - 1.
+    if (t >= 1 && t < NB) {
+        const int d = 31 - __clz(t);
+        const int io = (2 * (t - (1 << d)) + 1) * (1 << (7 - d)) - 1;
+        out->tree[t] = uniq[io];
+    } else {
+        out->tree[0] = KeyMax<K>::value;
+    }
+    out->uniq[t] = uniq[t];
+    // masks
+    const unsigned bal_eq = __ballot_sync(0xFFFFFFFFu, my_eq != 0);
+    if ((t & 31) == 0) out->eq_mask[t >> 5] = bal_eq;
+    __shared__ uint32_t beq[NB / 32];
+    if (t < NB / 32) beq[t] = 0;
+    __syncthreads();
+    if (my_eq) atomicOr(&beq[(range_id + 1) >> 5], 1u << ((range_id + 1) & 31));
+    __syncthreads();
+    if (t < NB / 32) out->bucket_eq[t] = beq[t];
+    if (t == 0) {
+        out->nbuckets = nbk;
+        out->has_eq = total_eq ? 1u : 0u;
+        out->nuniq = K_u;
+    }
+}
+
+// Bucket of key x under a split set held in shared memory.
+template <typename K>
+__device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x, bool has_eq,
+                                                const K* __restrict__ uniq, const uint8_t* __restrict__ range_b,
+                                                const uint8_t* __restrict__ eq_b, const uint32_t* __restrict__ eq_mask) {
+    uint32_t i = 1;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) i = 2 * i + (tree[i] < x ? 1u : 0u);
+    const uint32_t j = i - 256;  // number of unique splitters < x
+    if (!has_eq) return j;
+    if (j < 255 && ((eq_mask[j >> 5] >> (j & 31)) & 1u) && uniq[j] == x) return eq_b[j];
+    return range_b[j];
+}
+
+// ===========================================================================
+// 4. The partition pass (persistent; tiles claimed in order)
+
+template <typename K>
+struct PartArgs {
+    const SegDesc* segs;
+    const uint32_t* tile_seg;     // global tile -> segment (nullptr: single segment 0)
+    const SplitSet<K>* splits;
+    K* out;                       // level output buffer
+    unsigned long long* status;   // ntiles * NB
+    uint64_t* bucket_counts;      // nsegs * NB, written by each segment's last tile
+    LevelCtl* ctl;
+    uint32_t ntiles;              // used when ntiles_dev is null
+    const uint32_t* ntiles_dev;   // tile count written by prepare_level_kernel
+};
+
+template <typename K, int THREADS, int IPT>
+struct PartSmem {
+    K keys[THREADS * IPT];
+    uint8_t bkt[THREADS * IPT];
+    K tree[NB];
+    K uniq[NB];
+    uint64_t region_off[NB];
+    uint64_t region_cap[NB];
+    uint64_t gdelta[NB];
+    uint32_t hist[NB];
+    uint32_t loc[NB];
+    uint32_t wtot[8];
+    uint8_t range_b[NB];
+    uint8_t eq_b[NB];
+    uint32_t eq_mask[NB / 32];
+    uint8_t ovf[NB];
+    uint32_t tile, seg, has_eq, nbk;
+};
+
+template <typename K, typename InCodec, int THREADS, int IPT>
+__global__ void __launch_bounds__(THREADS) partition_kernel(PartArgs<K> a, InCodec in) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using SM = PartSmem<K, THREADS, IPT>;
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
+    constexpr int TILE = THREADS * IPT;
+    const int tid = threadIdx.x;
+    uint32_t cached_seg = 0xFFFFFFFFu;
+    const uint32_t ntiles = a.ntiles_dev ? *a.ntiles_dev : a.ntiles;
+
+    for (int b = tid; b < NB; b += THREADS) sm.hist[b] = 0;
+
+    while (true) {
+        if (tid == 0) sm.tile = atomicAdd(&a.ctl->tile_counter, 1u);
+        __syncthreads();
+        const uint32_t t = sm.tile;
+        if (t >= ntiles) break;
+        const uint32_t seg = a.tile_seg ? a.tile_seg[t] : 0u;
+        const SegDesc sd = a.segs[seg];
+        if (seg != cached_seg) {
+            const SplitSet<K>& ss = a.splits[seg];
+            for (int b = tid; b < NB; b += THREADS) {
+                sm.tree[b] = ss.tree[b];
+                sm.uniq[b] = ss.uniq[b];
+                sm.region_off[b] = ss.region_off[b];
+                sm.region_cap[b] = ss.region_cap[b];
+                sm.range_b[b] = ss.range_b[b];
+                sm.eq_b[b] = ss.eq_b[b];
+            }
+            if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
+            if (tid == 0) {
+                sm.has_eq = ss.has_eq;
+                sm.nbk = ss.nbuckets;
+            }
+            cached_seg = seg;
+        }
+        __syncthreads();
+        const uint32_t ti = t - sd.tile_start;
+        const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
+        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const bool has_eq = sm.has_eq != 0;
+
+        // load (striped: element r*THREADS + tid) and classify
+        K key[IPT];
+        uint32_t br[IPT];  // bucket | rank << 8
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t idx = (uint32_t)(r * THREADS + tid);
+            if (idx < cnt) key[r] = in.load(base + idx);
+        }
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t idx = (uint32_t)(r * THREADS + tid);
+            const bool valid = idx < cnt;
+            // every lane takes part in the warp votes below; lanes past the end
+            // of the tile carry the out-of-range bucket NB
+            const uint32_t b = valid ? find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask)
+                                     : (uint32_t)NB;
+            // warp-uniform bucket (sorted / few-distinct input): one atomic for the warp
+            const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, b, 0);
+            const bool uni = __all_sync(0xFFFFFFFFu, b == b0);
+            uint32_t rank = 0;
+            if (uni) {
+                if (b0 < (uint32_t)NB) {
+                    uint32_t basev = 0;
+                    if (lane_id() == 0) basev = atomicAdd(&sm.hist[b0], 32u);
+                    rank = __shfl_sync(0xFFFFFFFFu, basev, 0) + lane_id();
+                }
+            } else if (valid) {
+                rank = atomicAdd(&sm.hist[b], 1u);
+            }
+            br[r] = b | (rank << 8);
+        }
+        __syncthreads();
+
+        // publish this tile's aggregate (or its inclusive prefix if first in segment)
+        uint32_t h = 0;
+        if (tid < NB) {
+            h = sm.hist[tid];
+            const unsigned long long w = (ti == 0 ? ST_INC : ST_AGG) | (unsigned long long)h;
+            st_release(&a.status[(size_t)t * NB + tid], w);
+        }
+        const uint32_t excl = block_exclusive_scan_first<NB, uint32_t>(h, sm.wtot, (uint32_t*)nullptr);
+        if (tid < NB) sm.loc[tid] = excl;
+        __syncthreads();
+
+        // stage keys into shared memory in bucket order
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t idx = (uint32_t)(r * THREADS + tid);
+            if (idx < cnt) {
+                const uint32_t b = br[r] & 0xFFu;
+                const uint32_t p = sm.loc[b] + (br[r] >> 8);
+                sm.keys[p] = key[r];
+                sm.bkt[p] = (uint8_t)b;
+            }
+        }
+
+        // decoupled look-back: one thread per bucket
+        if (tid < NB) {
+            uint64_t prefix = 0;
+            bool ok = true;
+            if (ti > 0) {
+                uint32_t p = t - 1;
+                while (true) {
+                    unsigned long long v;
+                    uint32_t spins = 0;
+                    while (true) {
+                        v = ld_acquire(&a.status[(size_t)p * NB + tid]);
+                        if (v & (ST_INC | ST_AGG)) break;
+                        if (++spins > SPIN_LIMIT) break;
+                        __nanosleep(spins < 64 ? 20 : 200);
+                    }
+                    if (!(v & (ST_INC | ST_AGG))) {
+                        ok = false;
+                        raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
+                        break;
+                    }
+                    prefix += v & ST_VAL;
+                    if (v & ST_INC) break;
+                    --p;
+                }
+                st_release(&a.status[(size_t)t * NB + tid], ST_INC | (unsigned long long)(prefix + h));
+            }
+            const uint64_t end = prefix + h;
+            const bool ovf = !ok || end > sm.region_cap[tid];
+            if (ovf && h) raise_error(&a.ctl->err, ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
+            sm.ovf[tid] = ovf ? 1 : 0;
+            sm.gdelta[tid] = sd.out_base + sm.region_off[tid] + prefix - (uint64_t)sm.loc[tid];
+            if (ti == sd.ntiles - 1) a.bucket_counts[(size_t)seg * NB + tid] = end;
+        }
+        __syncthreads();
+
+        // coalesced write-out
+        for (uint32_t i = tid; i < cnt; i += THREADS) {
+            const uint32_t b = sm.bkt[i];
+            if (!sm.ovf[b]) a.out[sm.gdelta[b] + i] = sm.keys[i];
+        }
+        if (tid < NB) sm.hist[tid] = 0;
+        __syncthreads();
+    }
+}
+
+// Exact histogram of a level (the fallback after a capacity overflow).
+template <typename K, typename InCodec, int THREADS, int IPT>
+__global__ void __launch_bounds__(THREADS) count_kernel(PartArgs<K> a, InCodec in) {
+    __shared__ K tree[NB];
+    __shared__ K uniq[NB];
+    __shared__ uint8_t range_b[NB], eq_b[NB];
+    __shared__ uint32_t eq_mask[NB / 32];
+    __shared__ uint32_t hist[NB];
+    __shared__ uint32_t has_eq;
+    constexpr int TILE = THREADS * IPT;
+    const uint32_t ntiles = a.ntiles_dev ? *a.ntiles_dev : a.ntiles;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint32_t seg = a.tile_seg ? a.tile_seg[t] : 0u;
+        const SegDesc sd = a.segs[seg];
+        const SplitSet<K>& ss = a.splits[seg];
+        for (int b = threadIdx.x; b < NB; b += THREADS) {
+            tree[b] = ss.tree[b];
+            uniq[b] = ss.uniq[b];
+            range_b[b] = ss.range_b[b];
+            eq_b[b] = ss.eq_b[b];
+            hist[b] = 0;
+        }
+        if (threadIdx.x < NB / 32) eq_mask[threadIdx.x] = ss.eq_mask[threadIdx.x];
+        if (threadIdx.x == 0) has_eq = ss.has_eq;
+        __syncthreads();
+        const uint32_t ti = t - sd.tile_start;
+        const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
+        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        for (uint32_t i = threadIdx.x; i < cnt; i += THREADS) {
+            const K x = in.load(base + i);
+            atomicAdd(&hist[find_bucket<K>(tree, x, has_eq != 0, uniq, range_b, eq_b, eq_mask)], 1u);
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b < NB; b += THREADS)
+            if (hist[b]) atomicAdd((unsigned long long*)&a.bucket_counts[(size_t)seg * NB + b],
+                                   (unsigned long long)hist[b]);
+        __syncthreads();
+    }
+}
+
+// Re-lay the bucket regions of every segment from exact counts.
+template <typename K>
+__global__ void __launch_bounds__(NB) exact_regions_kernel(SplitSet<K>* splits, const uint64_t* bucket_counts,
+                                                           uint32_t nsegs) {
+    __shared__ uint64_t wtot64[8];
+    const uint32_t s = blockIdx.x;
+    if (s >= nsegs) return;
+    const uint64_t c = bucket_counts[(size_t)s * NB + threadIdx.x];
+    const uint64_t cap = (c + 15) & ~15ull;
+    const uint64_t off = block_exclusive_scan_first<NB, uint64_t>(cap, wtot64, (uint64_t*)nullptr);
+    splits[s].region_off[threadIdx.x] = off;
+    splits[s].region_cap[threadIdx.x] = cap;
+}
+
+// ===========================================================================
+// 5. Planning: classify each bucket of each segment (one block per segment)
+
+template <typename K>
+struct PlanArgs {
+    const SegDesc* segs;
+    const SplitSet<K>* splits;
+    const uint64_t* bucket_counts;
+    const K* level_out;                 // the level's output buffer
+    LeafItem<K>* items[NCLASS + 1];     // per class, plus the copy list
+    uint32_t item_cap;
+    SegDesc* next;                      // next-level segments (in_off into level_out)
+    uint32_t next_cap;
+    LevelCtl* ctl;
+    int key_bytes;
+};
+
+template <typename K>
+__global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs) {
+    __shared__ uint64_t wtot64[8];
+    const uint32_t s = blockIdx.x;
+    if (s >= nsegs) return;
+    const SegDesc sd = a.segs[s];
+    const SplitSet<K>& ss = a.splits[s];
+    const int b = threadIdx.x;
+    const uint64_t c = (b < (int)ss.nbuckets) ? a.bucket_counts[(size_t)s * NB + b] : 0ull;
+    const uint64_t excl = block_exclusive_scan_first<NB, uint64_t>(c, wtot64, (uint64_t*)nullptr);
+    if (c == 0) return;
+    atomicMax(&a.ctl->max_bucket, (uint32_t)(c > 0xFFFFFFFFull ? 0xFFFFFFFFull : c));
+    atomicAdd(&a.ctl->nonempty, 1u);
+    atomicAdd((unsigned long long*)&a.ctl->level_keys, (unsigned long long)c);
+    const K* src = a.level_out + sd.out_base + ss.region_off[b];
+    const uint64_t dst = sd.final_off + excl;
+    const bool is_eq = (ss.bucket_eq[b >> 5] >> (b & 31)) & 1u;
+    if (is_eq || c == 1) {
+        for (uint64_t o = 0; o < c; o += COPY_CHUNK) {
+            const uint32_t slot = atomicAdd(&a.ctl->n_items[CLS_COPY], 1u);
+            if (slot < a.item_cap) {
+                LeafItem<K> it;
+                it.src = src + o;
+                it.dst = dst + o;
+                it.count = (uint32_t)((c - o) < COPY_CHUNK ? (c - o) : COPY_CHUNK);
+                it.pad_ = 0;
+                a.items[CLS_COPY][slot] = it;
+            } else {
+                raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
+            }
+        }
+    } else if (c <= leaf_max(a.key_bytes)) {
+        const int cls = class_of(a.key_bytes, (uint32_t)c);
+        const uint32_t slot = atomicAdd(&a.ctl->n_items[cls], 1u);
+        if (slot < a.item_cap) {
+            LeafItem<K> it;
+            it.src = src;
+            it.dst = dst;
+            it.count = (uint32_t)c;
+            it.pad_ = 0;
+            a.items[cls][slot] = it;
+        } else {
+            raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
+        }
+    } else {
+        const uint32_t slot = atomicAdd(&a.ctl->n_next, 1u);
+        if (slot < a.next_cap) {
+            SegDesc n;
+            n.in_off = sd.out_base + ss.region_off[b];
+            n.count = c;
+            n.final_off = dst;
+            n.out_base = 0;
+            n.tile_start = 0;
+            n.ntiles = 0;
+            a.next[slot] = n;
+            atomicAdd((unsigned long long*)&a.ctl->next_keys, (unsigned long long)c);
+        } else {
+            raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
+        }
+    }
+}
+
+// Give the next level's segments their tiles and output regions (one block).
+__global__ void __launch_bounds__(1024) prepare_level_kernel(SegDesc* segs, uint32_t nsegs, uint32_t tile,
+                                                             LevelCtl* ctl_next) {
+    __shared__ uint64_t wt1[32], wt2[32];
+    __shared__ uint64_t tot1, tot2;
+    __shared__ uint64_t carry_tiles, carry_bound;
+    if (threadIdx.x == 0) {
+        carry_tiles = 0;
+        carry_bound = 0;
+    }
+    __syncthreads();
+    for (uint32_t base = 0; base < nsegs; base += 1024) {
+        const uint32_t s = base + threadIdx.x;
+        uint64_t nt = 0, bd = 0;
+        if (s < nsegs) {
+            nt = (segs[s].count + tile - 1) / tile;
+            bd = (region_bound(segs[s].count) + 15) & ~15ull;
+        }
+        const uint64_t ex_t = block_exclusive_scan_first<1024, uint64_t>(nt, wt1, &tot1);
+        const uint64_t ex_b = block_exclusive_scan_first<1024, uint64_t>(bd, wt2, &tot2);
+        if (s < nsegs) {
+            segs[s].tile_start = (uint32_t)(carry_tiles + ex_t);
+            segs[s].ntiles = (uint32_t)nt;
+            segs[s].out_base = carry_bound + ex_b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry_tiles += tot1;
+            carry_bound += tot2;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ctl_next->ntiles_next = (uint32_t)carry_tiles;
+        ctl_next->bound_next = carry_bound;
+    }
+}
+
+// tile -> segment map (one block per segment)
+__global__ void tile_map_kernel(const SegDesc* segs, uint32_t nsegs, uint32_t* tile_seg) {
+    const uint32_t s = blockIdx.x;
+    if (s >= nsegs) return;
+    const SegDesc sd = segs[s];
+    for (uint32_t i = threadIdx.x; i < sd.ntiles; i += blockDim.x) tile_seg[sd.tile_start + i] = s;
+}
+
+// ===========================================================================
+// 6. Leaves
+
+// One warp per bucket of at most 32*IPT keys (class 0).
+template <typename K, typename OutCodec, int IPT>
+__global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
+                                                        OutCodec out) {
+    __shared__ K stage[8][32 * IPT];
+    const unsigned warp = threadIdx.x >> 5, lane = lane_id();
+    K* sw = stage[warp];
+    for (uint32_t it = blockIdx.x * 8 + warp; it < nitems; it += gridDim.x * 8) {
+        const LeafItem<K> item = items[it];
+        for (uint32_t i = lane; i < 32 * IPT; i += 32) sw[i] = i < item.count ? item.src[i] : KeyMax<K>::value;
+        __syncwarp();
+        K x[IPT];
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) x[r] = sw[lane * IPT + r];
+        __syncwarp();
+        warp_bitonic_sort<K, IPT>(x);
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) sw[lane * IPT + r] = x[r];
+        __syncwarp();
+        for (uint32_t i = lane; i < item.count; i += 32) out.store(item.dst + i, sw[i]);
+        __syncwarp();
+    }
+}
+
+// One block per bucket of at most THREADS*IPT keys.
+template <typename K, typename OutCodec, int THREADS, int IPT>
+__global__ void __launch_bounds__(THREADS) leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
+                                                             OutCodec out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* smem = reinterpret_cast<K*>(smem_raw);
+    constexpr int N = THREADS * IPT;
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const LeafItem<K> item = items[it];
+        for (uint32_t i = threadIdx.x; i < N; i += THREADS) smem[i] = i < item.count ? item.src[i] : KeyMax<K>::value;
+        __syncthreads();
+        K x[IPT];
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
+        __syncthreads();
+        block_bitonic_sort<K, THREADS, IPT>(x, smem);
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) out.store(item.dst + i, smem[i]);
+        __syncthreads();
+    }
+}
+
+// Copy equality buckets (and single keys) to their final place.
+template <typename K, typename OutCodec>
+__global__ void __launch_bounds__(256) leaf_copy_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
+                                                        OutCodec out) {
+    for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
+        const LeafItem<K> item = items[it];
+        for (uint32_t i = threadIdx.x; i < item.count; i += 256) out.store(item.dst + i, item.src[i]);
+    }
+}
+
+// ===========================================================================
+// 7. Whole arrays that fit one leaf: sort straight from and to the caller's layout.
+
+template <typename InCodec, typename OutCodec, int IPT>
+__global__ void __launch_bounds__(32) small_warp_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
+    using K = typename InCodec::Key;
+    __shared__ K sw[32 * IPT];
+    const unsigned lane = lane_id();
+    for (uint32_t i = lane; i < 32 * IPT; i += 32) sw[i] = i < n ? in.load(i) : KeyMax<K>::value;
+    __syncwarp();
+    K x[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) x[r] = sw[lane * IPT + r];
+    __syncwarp();
+    warp_bitonic_sort<K, IPT>(x);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) sw[lane * IPT + r] = x[r];
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) out.store(i, sw[i]);
+}
+
+template <typename InCodec, typename OutCodec, int THREADS, int IPT>
+__global__ void __launch_bounds__(THREADS) small_block_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
+    using K = typename InCodec::Key;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* smem = reinterpret_cast<K*>(smem_raw);
+    constexpr int N = THREADS * IPT;
+    for (uint32_t i = threadIdx.x; i < N; i += THREADS) smem[i] = i < n ? in.load(i) : KeyMax<K>::value;
+    __syncthreads();
+    K x[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
+    __syncthreads();
+    block_bitonic_sort<K, THREADS, IPT>(x, smem);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) out.store(i, smem[i]);
+}
+
+}  // namespace s512

@@ -1,0 +1,403 @@
+"""Benchmark: in-place sort of 2^28 doubles (uniform [0,1)) on one B200.
+
+One step = one Sort512::Sort of a fresh 2^28-double array resident in HBM
+(a distinct input per step, 2 GiB each, so every step reads from DRAM, not
+L2).  `value` is device throughput in Gkeys/s (CUDA events on the launching
+stream, max over ranks); `e2e` is the same sort through the C ABI with a
+pinned HOST buffer (host->device copy, sort, device->host copy inside the
+timed region).  `roofline` reports the dominant kernel against the measured
+HBM copy bandwidth, `cpu_baseline` the reference's own CPU sort on this host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With --gpus N > 1 (torchrun) every rank sorts its own array: replicas, no
+collective on the data path ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "avx-512-sort_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+sys.path.insert(0, PKG)
+
+METRIC = "Gkeys/s at 2^28 int32/f64/kv; learned vs plain splitters; % of HBM roofline"
+N_KEYS = 1 << 28
+WORKLOAD = "Sort512::Sort, double, n=2^28, uniform [0,1) (splitmix64 seed per step), sampled splitters"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_KEYS)
+    ap.add_argument("--no-extras", action="store_true", help="skip the per-distribution / int32 / kv extras")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+
+        def rd():
+            for line in self.proc.stdout:
+                self.samples.append([x.strip() for x in line.split(",")])
+
+        self.thread = threading.Thread(target=rd, daemon=True)
+        self.thread.start()
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm = []
+        smax = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                smax = float(s[2])
+                for nm, val in zip(names, s[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        sm.sort()
+        med = sm[len(sm) // 2] if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_sort(n: int, threads: int, fn: str = "sort_omp_partition", dtype="f64", seed=1):
+    """Time the reference (compiled in place) or, without AVX-512, the C
+    restatement, on `n` keys of the workload.  Returns (seconds, kind, cores)."""
+    sys.path.insert(0, ORACLE_DIR)
+    import numpy as np
+
+    import workloads
+    from oracle import REF_SO, Oracle, Reference, cpu_has_avx512
+    a = workloads.uniform01_np(n, seed) if dtype == "f64" else workloads.uniform_i32_np(n, seed)
+    if os.path.exists(REF_SO) and cpu_has_avx512():
+        ref = Reference()
+        ref.set_threads(threads)
+        t0 = time.perf_counter()
+        ref.call(fn, a)
+        dt = time.perf_counter() - t0
+        kind, cores = "reference", (threads if fn != "sort" else 1)
+    else:
+        o = Oracle()
+        t0 = time.perf_counter()
+        o.sort(a)
+        dt = time.perf_counter() - t0
+        kind, cores = "port", 1
+    assert bool(np.all(a[1:] >= a[:-1]))
+    return dt, kind, cores
+
+
+def run_reference_arm(args, world, rank):
+    """--impl reference: the reference's own CPU sort on this host's cores."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n = min(args.n, 1 << 26)  # bounded sample of the 2^28 workload per step
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference_sort(1 << 20, threads)
+    times = []
+    kind, cores = "port", 1
+    for s in range(args.steps):
+        dt, kind, cores = cpu_reference_sort(n, threads, seed=100 + s)
+        times.append(dt)
+    tot = sum(times)
+    val = n * len(times) / tot / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "Gkeys/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / len(times) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": args.n, "sample_n_per_step": n,
+                   "function": "Sort512::SortOmpPartition" if kind == "reference" else "restated CoreSort"},
+        "cpu_baseline": {"value": round(val, 4), "unit": "Gkeys/s", "cores": cores, "kind": kind,
+                         "sample": f"{n} uniform doubles per step, {args.steps} steps"},
+        "e2e": {"value": round(val, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+
+    import sort512cuda as s512
+    import workloads
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    s512.lib()
+    n = args.n
+    stream = torch.cuda.current_stream(dev)
+    s512.set_config(collect_stats=1)
+
+    def make(seed):
+        return workloads.uniform01_torch(n, seed=seed + 1000 * rank, device=dev)
+
+    # warm-up (untimed)
+    for w in range(args.warmup):
+        x = make(900 + w)
+        s512.sort(x, flags=s512.ASYNC, stream=stream)
+        torch.cuda.synchronize()
+        assert bool((x[1:] >= x[:-1]).all()), "warm-up output not sorted"
+        del x
+    # distinct inputs for every timed step, generated before timing
+    inputs = [make(s) for s in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier(world)
+
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    part_ms, part_keys, leaf_ms, samp_ms, launches, levels = [], [], [], [], 0, 0
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0.record(stream)
+    for s in range(args.steps):
+        s512.sort(inputs[s], flags=s512.ASYNC, stream=stream)
+        st = s512.stats()
+        part_ms.append(sum(st["partition_ms"]))
+        part_keys.append(sum(st["partition_keys"]))
+        leaf_ms.append(sum(st["leaf_ms"]))
+        samp_ms.append(sum(st["sample_ms"]))
+        launches += st["kernel_launches"]
+        levels = st["levels"]
+        last = st
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clocks = sampler.stop() if sampler else None
+    dev_ms = ev0.elapsed_time(ev1)
+    dev_ms = max_over_ranks(dev_ms, world)
+    ok = all(bool((x[1:] >= x[:-1]).all()) for x in inputs)
+    del inputs
+    torch.cuda.empty_cache()
+    ms_per_step = dev_ms / args.steps
+    value = n * world / (ms_per_step * 1e-3) / 1e9
+
+    # roofline of the partition kernel: algorithmic bytes = read + write of
+    # every key it moves (8 B per double), per launch
+    peak, peak_kind = peaks()
+    tot_part_ms = sum(part_ms)
+    tot_leaf_ms = sum(leaf_ms)
+    part_bytes = 2 * 8 * sum(part_keys)
+    part_gbs = part_bytes / (tot_part_ms * 1e-3) / 1e9 if tot_part_ms > 0 else None
+    leaf_bytes = 2 * 8 * n * args.steps
+    leaf_gbs = leaf_bytes / (tot_leaf_ms * 1e-3) / 1e9 if tot_leaf_ms > 0 else None
+    dominant = "partition" if tot_part_ms >= tot_leaf_ms else "leaf"
+    ach = part_gbs if dominant == "partition" else leaf_gbs
+    roofline = {"bound": "hbm", "kernel": "partition_kernel" if dominant == "partition" else "leaf sorts",
+                "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4) if ach else None, "peak_source": peak_kind,
+                "traffic": None,
+                "partition_kernel": {"achieved": round(part_gbs, 1) if part_gbs else None,
+                                     "frac": round(part_gbs / peak, 4) if part_gbs else None,
+                                     "ms_per_step": round(tot_part_ms / args.steps, 3),
+                                     "launches_per_step": levels,
+                                     "algorithmic_bytes_per_step": part_bytes // args.steps},
+                "leaf_sorts": {"achieved": round(leaf_gbs, 1) if leaf_gbs else None,
+                               "frac": round(leaf_gbs / peak, 4) if leaf_gbs else None,
+                               "ms_per_step": round(tot_leaf_ms / args.steps, 3)},
+                "sampling_ms_per_step": round(sum(samp_ms) / args.steps, 3)}
+    if rank != 0:
+        return
+
+    # e2e through the C ABI with a pinned host buffer
+    e2e = None
+    try:
+        import numpy as np
+        host_src = workloads.uniform01_torch(n, seed=4242, device=dev).cpu()
+        host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        e_times = []
+        for s in range(max(2, min(args.steps, 3)) + 1):
+            host.copy_(host_src)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s512.sort(host.numpy())  # host pointer: H2D, sort, D2H, then return
+            t1 = time.perf_counter()
+            if s > 0:
+                e_times.append(t1 - t0)
+        hv = host.numpy()
+        assert bool(np.all(hv[1:] >= hv[:-1]))
+        e_ms = sum(e_times) / len(e_times) * 1e3
+        e2e = {"value": round(n / (e_ms * 1e-3) / 1e9, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": n * 8,
+               "d2h_bytes_per_step": n * 8, "ms_per_step": round(e_ms, 3),
+               "timing": "host wall clock around the blocking C-ABI call (pinned host buffer)"}
+        del host, host_src
+    except Exception as e:  # noqa: BLE001
+        e2e = {"value": None, "unit": "Gkeys/s", "error": str(e)[:200]}
+
+    # CPU baseline: the reference's SortOmpPartition on all host cores
+    cpu = None
+    if not args.no_cpu:
+        try:
+            threads = os.cpu_count() or 1
+            sn = 1 << 26
+            dt, kind, cores = cpu_reference_sort(sn, threads)
+            cpu = {"value": round(sn / dt / 1e9, 4), "unit": "Gkeys/s", "cores": cores, "kind": kind,
+                   "sample": f"Sort512::SortOmpPartition on {sn} uniform doubles (one run)" if kind == "reference"
+                   else f"restated CoreSort on {sn} uniform doubles, 1 core"}
+        except Exception as e:  # noqa: BLE001
+            cpu = {"value": None, "unit": "Gkeys/s", "error": str(e)[:200]}
+
+    extras = {}
+    if not args.no_extras:
+        extras = run_extras(n, dev, stream)
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Gkeys/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": n, "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "l2": "inputs larger than L2: a distinct 2 GiB input per step",
+                   "levels": levels},
+        "clocks": clocks, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+        "gpu_launches": launches, "sorted_ok": ok, "stats_last_step": last, "extras": extras,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_extras(n, dev, stream):
+    """One timed run per extra workload (reported beside the headline)."""
+    import torch
+
+    import sort512cuda as s512
+    import workloads
+    out = {}
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    for dist in workloads.DOUBLE_DISTS:
+        x = workloads.double_dist_torch(dist, n, seed=5, device=dev)
+        s512.sort(x, flags=s512.ASYNC, stream=stream)  # warm
+        x = workloads.double_dist_torch(dist, n, seed=6, device=dev)
+        ms = timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream))
+        ok = bool((x[1:] >= x[:-1]).all())
+        st = s512.stats()
+        out[f"f64_{dist}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "sorted": ok,
+                              "levels": st["levels"], "fallbacks": st["fallbacks"]}
+        del x
+    x = workloads.uniform_i32_torch(n, seed=8, device=dev)
+    s512.sort(x.clone(), flags=s512.ASYNC, stream=stream)
+    ms = timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream))
+    out["i32_uniform"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
+                          "sorted": bool((x[1:] >= x[:-1]).all())}
+    del x
+    for kname in ("uniform", "zipf"):
+        k = workloads.uniform_i32_torch(n, 9, dev) if kname == "uniform" else workloads.zipf_i32_torch(n, seed=9,
+                                                                                                         device=dev)
+        v = torch.arange(n, dtype=torch.int32, device=dev)
+        s512.sort_kv(k.clone(), v.clone(), flags=s512.ASYNC, stream=stream)
+        ms = timed(lambda: s512.sort_kv(k, v, flags=s512.ASYNC, stream=stream))
+        out[f"kv_{kname}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
+                              "sorted": bool((k[1:] >= k[:-1]).all())}
+        del k, v
+    torch.cuda.empty_cache()
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

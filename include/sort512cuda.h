@@ -1,0 +1,142 @@
+/*
+ * sort512cuda.h -- C ABI of libsort512cuda, a B200 (sm_100a) implementation of
+ * the sorting path of berenger-eu/avx-512-sort.
+ *
+ * Plain pointers and sizes only.  Every function returns an int status
+ * (S512_OK == 0).  Pointers may be host or device memory: with S512_PTR_AUTO
+ * (the default) the library asks the CUDA driver which one it is; host data is
+ * copied to the device, sorted there and copied back before the call returns.
+ * Device data is sorted in place on `stream` (a cudaStream_t, NULL = the
+ * default stream); the call waits for the result unless S512_ASYNC is set.
+ *
+ * Every operation is in place, like the reference.  Scratch memory comes from
+ * a per-device pool that grows on demand and is kept until
+ * s512_release_scratch() or process exit.
+ *
+ * Element types: int32 ("i32"), double ("f64") and int32 key + int32 value
+ * pairs held in two arrays ("kv_i32").  Results:
+ *   - i32: the sorted array (bit-exact with the reference's Sort);
+ *   - f64: sorted by IEEE total order (-0.0 before +0.0, NaNs at the ends by
+ *     sign bit); for finite inputs this is bit-exact with the reference
+ *     except for the relative order of -0.0 and +0.0, which the reference
+ *     leaves to min/max operand order;
+ *   - kv: keys bit-exact, pairs ordered by (key, value).  The reference is
+ *     not stable, so only the (key, value) multiset is comparable.
+ */
+#ifndef SORT512CUDA_H
+#define SORT512CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define S512_API __attribute__((visibility("default")))
+#else
+#define S512_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    S512_OK = 0,
+    S512_ERR_ARG = 1,         /* bad argument (null pointer with n > 0, left > right, ...) */
+    S512_ERR_ALLOC = 2,       /* device or pinned allocation failed */
+    S512_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up (look-back spin) */
+    S512_ERR_CUDA = 4,        /* a CUDA runtime call failed; see s512_last_error_string() */
+    S512_ERR_INTERNAL = 5,    /* an internal capacity check failed */
+    S512_ERR_UNSUPPORTED = 6  /* no usable sm_100 device */
+};
+
+/* flags (bitwise or) */
+enum {
+    S512_PTR_AUTO = 0,        /* ask the driver whether pointers are host or device memory */
+    S512_PTR_HOST = 1,        /* pointers are host memory (pageable or pinned) */
+    S512_PTR_DEVICE = 2,      /* pointers are device memory */
+    S512_SPLIT_AUTO = 0,      /* splitter mode from s512_config (default: plain) */
+    S512_SPLIT_PLAIN = 4,     /* sampled splitters + binary search */
+    S512_SPLIT_LEARNED = 8,   /* learned monotone CDF model, plain splitters as fallback */
+    S512_ASYNC = 16           /* device pointers: return without waiting for the stream */
+};
+
+/* library configuration (process wide) */
+typedef struct s512_config {
+    int splitter_mode;        /* S512_SPLIT_PLAIN (default) or S512_SPLIT_LEARNED */
+    int collect_stats;        /* 1: time every phase with CUDA events (s512_get_stats) */
+    double max_imbalance;     /* learned model is rejected if max bucket > this x mean (default 3.0) */
+    uint64_t seed;            /* sampling seed (default 0x5EED) */
+} s512_config;
+
+/* per-call statistics of the last call on this host thread */
+#define S512_MAX_LEVELS 8
+typedef struct s512_stats {
+    double total_ms;                        /* device time of the whole call */
+    double sample_ms[S512_MAX_LEVELS];      /* sampling + sample sort + splitters/model, per level */
+    double partition_ms[S512_MAX_LEVELS];   /* the multi-way partition kernel, per level */
+    double leaf_ms[S512_MAX_LEVELS];        /* planning + leaf sorts, per level */
+    uint64_t partition_keys[S512_MAX_LEVELS]; /* keys moved by the partition kernel, per level */
+    uint32_t partition_launches[S512_MAX_LEVELS];
+    uint32_t levels;                        /* partition levels run */
+    uint32_t fallbacks;                     /* levels redone with exact counts after an overflow */
+    uint32_t learned_levels;                /* levels routed by the learned model */
+    uint32_t learned_rejected;              /* learned models rejected (imbalance / overflow) */
+    double max_bucket_over_mean[S512_MAX_LEVELS]; /* bucket imbalance per level */
+    uint32_t kernel_launches;               /* kernels launched by the call */
+    uint32_t key_bytes;                     /* 4 or 8 */
+} s512_stats;
+
+/* --- configuration, errors, resources ---------------------------------- */
+S512_API int s512_set_config(const s512_config* cfg);
+S512_API int s512_get_config(s512_config* cfg);
+S512_API int s512_get_stats(s512_stats* out);
+S512_API const char* s512_last_error_string(void);
+S512_API int s512_release_scratch(void);
+S512_API int s512_version(void);
+
+/* --- Sort512::Sort<T,IndexType>(T array[], IndexType size)   sort512.hpp:5960-5964
+ *     Sort512::SortOmpPartition (sort512.hpp:5993-6004) maps here as well:
+ *     on the GPU the parallel backend is the device itself. */
+S512_API int s512_sort_i32(int* data, size_t n, int flags, void* stream);
+S512_API int s512_sort_f64(double* data, size_t n, int flags, void* stream);
+
+/* --- Sort512kv::Sort<T,IndexType>(T keys[], T values[], IndexType size)
+ *     sort512kv.hpp:6132-6136 (and SortOmpPartition, sort512kv.hpp:6165) */
+S512_API int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream);
+
+/* --- Sort512::Partition512<IndexType>(array, left, right, pivot)
+ *     int sort512.hpp:5729-5819, double 5821-5912; kv sort512kv.hpp:5959-6082.
+ *     Inclusive range [left, right]; elements <= pivot first.  *boundary
+ *     receives the index of the first element > pivot (right+1 if none). */
+S512_API int s512_partition_i32(int* data, size_t left, size_t right, int pivot, size_t* boundary,
+                       int flags, void* stream);
+S512_API int s512_partition_f64(double* data, size_t left, size_t right, double pivot, size_t* boundary,
+                       int flags, void* stream);
+S512_API int s512_partition_kv_i32(int* keys, int* values, size_t left, size_t right, int pivot,
+                          size_t* boundary, int flags, void* stream);
+
+/* --- Sort512::SmallSort16V(ptr, length)   int sort512.hpp:5312, double 2255
+ *     Sort512kv::SmallSort16V(keys, values, length)   sort512kv.hpp:5235
+ *     Lengths up to 16 vectors (256 int / 128 double / 256 pairs) run as one
+ *     warp; longer arrays (undefined in the reference) are fully sorted. */
+S512_API int s512_smallsort_i32(int* data, size_t len, int flags, void* stream);
+S512_API int s512_smallsort_f64(double* data, size_t len, int flags, void* stream);
+S512_API int s512_smallsort_kv_i32(int* keys, int* values, size_t len, int flags, void* stream);
+
+/* --- Sort512::CoreSmallSort / CoreSmallSort2..16 pointer forms
+ *     (sort512.hpp:95-97, 212, 282, ... 2211 double; 2722-2724 ... 5230 int;
+ *     sort512kv.hpp:179, 497, ... 5164): sort nvec consecutive vectors
+ *     (16 ints / 8 doubles / 16 pairs each), nvec in 1..16. */
+S512_API int s512_core_small_sort_i32(int* data, int nvec, int flags, void* stream);
+S512_API int s512_core_small_sort_f64(double* data, int nvec, int flags, void* stream);
+S512_API int s512_core_small_sort_kv_i32(int* keys, int* values, int nvec, int flags, void* stream);
+
+/* --- Sort512::popcount(__mmask16)   sort512.hpp:5714-5725 */
+S512_API int s512_popcount(unsigned mask);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SORT512CUDA_H */

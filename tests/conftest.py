@@ -1,0 +1,46 @@
+import json
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "avx-512-sort_b200")
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+for p in (PKG, ORACLE_DIR):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA sm_100 GPU (B200)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def golden():
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="session")
+def s512():
+    """The ctypes binding, with the library built if it is missing."""
+    import sort512cuda
+    if not os.path.exists(sort512cuda.LIB_PATH):
+        sort512cuda.build()
+    sort512cuda.lib()
+    return sort512cuda
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a CUDA device")
+    return torch.device("cuda:0")
