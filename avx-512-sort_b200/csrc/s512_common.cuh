@@ -5,7 +5,7 @@
 //   int32            -> uint32  k = x ^ 0x80000000            (signed order)
 //   double           -> uint64  k = x<0 ? ~bits : bits|2^63    (IEEE total order;
 //                                -0 sorts before +0, NaNs at the ends by sign)
-//   int key + int value (two arrays) -> uint64 k = (ukey << 32) | uint32(value)
+//   int key + int value (two arrays) -> uint64 k = (ukey << 32) | uvalue
 // The transform is applied where a kernel reads the caller's layout and undone
 // where it writes the caller's layout; every buffer in between holds encoded
 // keys.  The reference compares the same values with signed/ordered compares
@@ -54,8 +54,10 @@ __device__ __forceinline__ uint64_t dec_f64_bits(uint64_t k) {
     return (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
 }
 
+// key in the high half, value in the low half, both in signed order, so that
+// pairs sort by (key, value) -- the order the kv oracle uses for ties
 __device__ __forceinline__ uint64_t enc_kv(int key, int val) {
-    return ((uint64_t)enc_i32(key) << 32) | (uint32_t)val;
+    return ((uint64_t)enc_i32(key) << 32) | enc_i32(val);
 }
 
 // ---------------------------------------------------------------------------
@@ -98,7 +100,7 @@ struct CodecKV {
     __device__ __forceinline__ uint64_t load(size_t i) const { return enc_kv(__ldg(kin + i), __ldg(vin + i)); }
     __device__ __forceinline__ void store(size_t i, uint64_t k) const {
         kout[i] = dec_i32((uint32_t)(k >> 32));
-        vout[i] = (int)(uint32_t)k;
+        vout[i] = dec_i32((uint32_t)k);
     }
 };
 
