@@ -55,7 +55,7 @@ __device__ __forceinline__ uint64_t dec_f64_bits(uint64_t k) {
 }
 
 // key in the high half, value in the low half, both in signed order, so that
-// pairs sort by (key, value) -- the order the kv oracle uses for ties
+// pairs sort by (key, value) in lexicographic order
 __device__ __forceinline__ uint64_t enc_kv(int key, int val) {
     return ((uint64_t)enc_i32(key) << 32) | enc_i32(val);
 }

@@ -24,10 +24,10 @@ template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT
 // ---------------------------------------------------------------------------
 // leaf launches per class
 
-template <typename K, typename OutCodec, int THREADS, int IPT>
+template <typename K, typename OutCodec, int THREADS, int EPT>
 static int launch_leaf_block(DevCtx& C, const LeafItem<K>* items, uint32_t n, OutCodec out, cudaStream_t st) {
-    auto fn = leaf_block_kernel<K, OutCodec, THREADS, IPT>;
-    const size_t smem = (size_t)THREADS * IPT * sizeof(K);
+    auto fn = leaf_block_kernel<K, OutCodec, THREADS, EPT>;
+    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
     int grid = 0;
     S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
     fn<<<grid, THREADS, smem, st>>>(items, n, out);
@@ -39,7 +39,6 @@ template <typename K, typename OutCodec>
 static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint32_t n, OutCodec out,
                              cudaStream_t st) {
     if (n == 0) return S512_OK;
-    constexpr bool W = sizeof(K) == 4;
     switch (cls) {
         case 0: {
             auto fn = leaf_warp_kernel<K, OutCodec, 8>;
@@ -49,15 +48,11 @@ static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint3
             S512_LAUNCH_CHECK();
             return S512_OK;
         }
-        case 1: return launch_leaf_block<K, OutCodec, 64, 8>(C, items, n, out, st);
-        case 2: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, st);
-        case 3: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, st);
-        case 4: return W ? launch_leaf_block<K, OutCodec, 256, 16>(C, items, n, out, st)
-                         : launch_leaf_block<K, OutCodec, 512, 8>(C, items, n, out, st);
-        case 5: return W ? launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, st)
-                         : launch_leaf_block<K, OutCodec, 1024, 8>(C, items, n, out, st);
-        case 6: return W ? launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, st)
-                         : launch_leaf_block<K, OutCodec, 1024, 8>(C, items, n, out, st);
+        case 1: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, st);
+        case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, st);
+        case 3: return launch_leaf_block<K, OutCodec, 512, 8>(C, items, n, out, st);
+        case 4: return launch_leaf_block<K, OutCodec, 1024, 8>(C, items, n, out, st);
+        case 5: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, st);
         case CLS_COPY: {
             auto fn = leaf_copy_kernel<K, OutCodec>;
             int grid = 0;
@@ -72,11 +67,11 @@ static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint3
 }
 
 // Whole array in one leaf (n <= leaf_max).
-template <typename InCodec, typename OutCodec, int THREADS, int IPT>
+template <typename InCodec, typename OutCodec, int THREADS, int EPT>
 static int launch_small_block(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaStream_t st) {
     using K = typename InCodec::Key;
-    auto fn = small_block_sort_kernel<InCodec, OutCodec, THREADS, IPT>;
-    const size_t smem = (size_t)THREADS * IPT * sizeof(K);
+    auto fn = small_block_sort_kernel<InCodec, OutCodec, THREADS, EPT>;
+    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
     S512_CUDA_TRY(C.prepare((const void*)fn, smem));
     fn<<<1, THREADS, smem, st>>>(in, out, n);
     S512_LAUNCH_CHECK();
@@ -86,22 +81,17 @@ static int launch_small_block(DevCtx& C, InCodec in, OutCodec out, uint32_t n, c
 template <typename InCodec, typename OutCodec>
 static int sort_one_leaf(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaStream_t st) {
     using K = typename InCodec::Key;
-    constexpr bool W = sizeof(K) == 4;
     if (n <= 256) {
         small_warp_sort_kernel<InCodec, OutCodec, 8><<<1, 32, 0, st>>>(in, out, n);
         S512_LAUNCH_CHECK();
         return S512_OK;
     }
     switch (class_of(sizeof(K), n)) {
-        case 1: return launch_small_block<InCodec, OutCodec, 64, 8>(C, in, out, n, st);
-        case 2: return launch_small_block<InCodec, OutCodec, 128, 8>(C, in, out, n, st);
-        case 3: return launch_small_block<InCodec, OutCodec, 256, 8>(C, in, out, n, st);
-        case 4: return W ? launch_small_block<InCodec, OutCodec, 256, 16>(C, in, out, n, st)
-                         : launch_small_block<InCodec, OutCodec, 512, 8>(C, in, out, n, st);
-        case 5: return W ? launch_small_block<InCodec, OutCodec, 512, 16>(C, in, out, n, st)
-                         : launch_small_block<InCodec, OutCodec, 1024, 8>(C, in, out, n, st);
-        default: return W ? launch_small_block<InCodec, OutCodec, 1024, 16>(C, in, out, n, st)
-                          : launch_small_block<InCodec, OutCodec, 1024, 8>(C, in, out, n, st);
+        case 1: return launch_small_block<InCodec, OutCodec, 128, 8>(C, in, out, n, st);
+        case 2: return launch_small_block<InCodec, OutCodec, 256, 8>(C, in, out, n, st);
+        case 3: return launch_small_block<InCodec, OutCodec, 512, 8>(C, in, out, n, st);
+        case 4: return launch_small_block<InCodec, OutCodec, 1024, 8>(C, in, out, n, st);
+        default: return launch_small_block<InCodec, OutCodec, 1024, 16>(C, in, out, n, st);
     }
 }
 
@@ -149,13 +139,13 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
     S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
     const uint64_t seed = config().seed + 0x9E3779B97F4A7C15ull * (uint64_t)(level + 1);
-    sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed);
+    sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed, KB);
     S512_LAUNCH_CHECK();
     {
         auto fn = sample_sort_kernel<K>;
-        const size_t smem = (size_t)SAMPLE_N * KB;
+        const size_t smem = (size_t)padded_len(SAMPLE_N) * KB;
         S512_CUDA_TRY(C.prepare((const void*)fn, smem));
-        fn<<<nsegs, 1024, smem, st>>>(samples, nsegs);
+        fn<<<nsegs, 1024, smem, st>>>(samples, L.segs, nsegs, KB);
         S512_LAUNCH_CHECK();
     }
     splitter_kernel<K><<<nsegs, NB, 0, st>>>(samples, L.segs, nsegs, splits, KB);

@@ -25,7 +25,7 @@
 //     next partition level.
 #pragma once
 
-#include "s512_bitonic.cuh"
+#include "s512_blocksort.cuh"
 
 namespace s512 {
 
@@ -72,18 +72,18 @@ struct LeafItem {
     uint32_t pad_;
 };
 
-// Leaf size classes.  Class 0 is one warp per bucket; the others are one
-// block of THREADS x IPT keys per bucket.  COPY is for equality buckets.
-constexpr int NCLASS = 7;
+// Leaf size classes.  Class 0 is one warp per bucket (a 256-key bitonic
+// leaf); the others are one block per bucket (bitonic leaves + merge path,
+// s512_blocksort.cuh).  The copy list holds equality buckets.
+constexpr int NCLASS = 6;
 constexpr int CLS_COPY = NCLASS;  // index of the copy list
-__host__ __device__ constexpr int class_cap(int key_bytes, int c) {
-    // u32: 256 512 1024 2048 4096 8192 16384 ; u64: 256 512 1024 2048 4096 8192 (8192)
-    return key_bytes == 4 ? (256 << c) : (c >= 5 ? 8192 : (256 << c));
+__host__ __device__ constexpr int class_cap(int c) {
+    return c == 0 ? 256 : (512 << c);  // 256, 1024, 2048, 4096, 8192, 16384
 }
-__host__ __device__ constexpr uint32_t leaf_max(int key_bytes) { return key_bytes == 4 ? 16384u : 8192u; }
-__host__ __device__ inline int class_of(int key_bytes, uint32_t count) {
+__host__ __device__ constexpr uint32_t leaf_max(int /*key_bytes*/) { return 16384u; }
+__host__ __device__ inline int class_of(int /*key_bytes*/, uint32_t count) {
     int c = 0;
-    while (c < NCLASS - 1 && (uint32_t)class_cap(key_bytes, c) < count) ++c;
+    while (c < NCLASS - 1 && (uint32_t)class_cap(c) < count) ++c;
     return c;
 }
 
@@ -94,6 +94,16 @@ __host__ __device__ inline int target_buckets(int key_bytes, uint64_t count) {
     if (want < 2) want = 2;
     if (want > NB) want = NB;
     return (int)want;
+}
+
+// Keys sampled from a segment that will be split into nb buckets: about 128
+// per bucket (so a bucket's sample count is ~128 and its capacity bound ~1.6x
+// its expected size), between 2048 and SAMPLE_N.
+__host__ __device__ inline uint32_t sample_size(int nb) {
+    uint32_t m = 128u * (uint32_t)nb;
+    if (m < 2048u) m = 2048u;
+    if (m > (uint32_t)SAMPLE_N) m = SAMPLE_N;
+    return m;
 }
 
 // Upper bound of the total region capacity the splitter kernel may lay out
@@ -121,36 +131,29 @@ struct LevelCtl {
 
 template <typename Codec>
 __global__ void sample_kernel(Codec in, const SegDesc* __restrict__ segs, uint32_t nsegs,
-                              typename Codec::Key* __restrict__ samples, uint64_t seed) {
+                              typename Codec::Key* __restrict__ samples, uint64_t seed, int key_bytes) {
     const uint32_t s = blockIdx.x;
     if (s >= nsegs) return;
     const SegDesc sd = segs[s];
-    for (int i = threadIdx.x; i < SAMPLE_N; i += blockDim.x) {
+    const uint32_t m = sample_size(target_buckets(key_bytes, sd.count));
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
         const uint64_t h = mix64(seed ^ ((uint64_t)s << 32) ^ (uint64_t)i);
         const uint64_t pos = __umul64hi(h, sd.count);
         samples[(size_t)s * SAMPLE_N + i] = in.load(sd.in_off + pos);
     }
 }
 
-// 2. Sorting the samples: one block of 1024 threads x 16 keys per segment.
+// 2. Sorting the samples: one block of 1024 threads per segment.
 template <typename K>
-__global__ void __launch_bounds__(1024) sample_sort_kernel(K* __restrict__ samples, uint32_t nsegs) {
+__global__ void __launch_bounds__(1024) sample_sort_kernel(K* __restrict__ samples, const SegDesc* __restrict__ segs,
+                                                           uint32_t nsegs, int key_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* smem = reinterpret_cast<K*>(smem_raw);
-    constexpr int IPT = SAMPLE_N / 1024;
+    K* s = reinterpret_cast<K*>(smem_raw);
+    const uint32_t m = sample_size(target_buckets(key_bytes, segs[blockIdx.x].count));
     K* p = samples + (size_t)blockIdx.x * SAMPLE_N;
-    // coalesced load into shared memory, then the blocked register layout
-    for (int i = threadIdx.x; i < SAMPLE_N; i += 1024) smem[i] = p[i];
-    __syncthreads();
-    K x[IPT];
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
-    __syncthreads();
-    block_bitonic_sort<K, 1024, IPT>(x, smem);
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
-    __syncthreads();
-    for (int i = threadIdx.x; i < SAMPLE_N; i += 1024) p[i] = smem[i];
+    for (uint32_t i = threadIdx.x; i < m; i += 1024) s[pidx(i)] = p[i];
+    block_merge_sort<K, 1024, SAMPLE_N / 1024>(s, m);
+    for (uint32_t i = threadIdx.x; i < m; i += 1024) p[i] = s[pidx(i)];
 }
 
 // 3. Splitters and bucket regions: one block of 256 threads per segment.
@@ -194,10 +197,11 @@ __global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ sam
     const int t = threadIdx.x;
     const int nb = target_buckets(key_bytes, sd.count);
     const int ncand = nb - 1;
+    const uint32_t m = sample_size(nb);
 
     // candidate splitters at the sample quantiles
     K c = KeyMax<K>::value;
-    if (t < ncand) c = smp[(uint32_t)(((uint64_t)(t + 1) * SAMPLE_N) / nb) - 1];
+    if (t < ncand) c = smp[(uint32_t)(((uint64_t)(t + 1) * m) / nb) - 1];
     cand[t] = c;
     __syncthreads();
     const bool valid = t < ncand;
@@ -227,7 +231,7 @@ __global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ sam
     // sample counts per bucket -> capacities
     // range bucket j (t <= K_u): keys in (uniq[j-1], uniq[j]] or (uniq[j-1], uniq[j]) if eq_j
     uint64_t cap_range = 0, cap_eq = 0;
-    const double scale = (double)sd.count / (double)SAMPLE_N;
+    const double scale = (double)sd.count / (double)m;
     auto cap_of = [&](uint32_t cnt) -> uint64_t {
         double v = ((double)cnt + 6.0 * sqrt((double)cnt + 1.0) + 16.0) * scale;
         uint64_t cap = (uint64_t)ceil(v);
@@ -235,14 +239,14 @@ __global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ sam
         return (cap + 15) & ~15ull;
     };
     if (t <= (int)K_u) {
-        const uint32_t lo = (t == 0) ? 0u : upper_bound_dev<K>(smp, SAMPLE_N, uniq[t - 1]);
+        const uint32_t lo = (t == 0) ? 0u : upper_bound_dev<K>(smp, m, uniq[t - 1]);
         uint32_t hi;
-        if (t == (int)K_u) hi = SAMPLE_N;
-        else hi = my_eq ? lower_bound_dev<K>(smp, SAMPLE_N, uniq[t]) : upper_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
+        if (t == (int)K_u) hi = m;
+        else hi = my_eq ? lower_bound_dev<K>(smp, m, uniq[t]) : upper_bound_dev<K>(smp, m, uniq[t]);
         cap_range = cap_of(hi > lo ? hi - lo : 0u);
         if (my_eq) {
-            const uint32_t e0 = lower_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
-            const uint32_t e1 = upper_bound_dev<K>(smp, SAMPLE_N, uniq[t]);
+            const uint32_t e0 = lower_bound_dev<K>(smp, m, uniq[t]);
+            const uint32_t e1 = upper_bound_dev<K>(smp, m, uniq[t]);
             cap_eq = cap_of(e1 - e0);
         }
     }
@@ -684,26 +688,17 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
     }
 }
 
-// One block per bucket of at most THREADS*IPT keys.
-template <typename K, typename OutCodec, int THREADS, int IPT>
+// One block per bucket of at most THREADS*EPT keys.
+template <typename K, typename OutCodec, int THREADS, int EPT>
 __global__ void __launch_bounds__(THREADS) leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
                                                              OutCodec out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* smem = reinterpret_cast<K*>(smem_raw);
-    constexpr int N = THREADS * IPT;
+    K* s = reinterpret_cast<K*>(smem_raw);
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const LeafItem<K> item = items[it];
-        for (uint32_t i = threadIdx.x; i < N; i += THREADS) smem[i] = i < item.count ? item.src[i] : KeyMax<K>::value;
-        __syncthreads();
-        K x[IPT];
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
-        __syncthreads();
-        block_bitonic_sort<K, THREADS, IPT>(x, smem);
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) out.store(item.dst + i, smem[i]);
+        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) s[pidx(i)] = item.src[i];
+        block_merge_sort<K, THREADS, EPT>(s, item.count);
+        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) out.store(item.dst + i, s[pidx(i)]);
         __syncthreads();
     }
 }
@@ -739,23 +734,14 @@ __global__ void __launch_bounds__(32) small_warp_sort_kernel(InCodec in, OutCode
     for (uint32_t i = lane; i < n; i += 32) out.store(i, sw[i]);
 }
 
-template <typename InCodec, typename OutCodec, int THREADS, int IPT>
+template <typename InCodec, typename OutCodec, int THREADS, int EPT>
 __global__ void __launch_bounds__(THREADS) small_block_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
     using K = typename InCodec::Key;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* smem = reinterpret_cast<K*>(smem_raw);
-    constexpr int N = THREADS * IPT;
-    for (uint32_t i = threadIdx.x; i < N; i += THREADS) smem[i] = i < n ? in.load(i) : KeyMax<K>::value;
-    __syncthreads();
-    K x[IPT];
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) x[r] = smem[threadIdx.x * IPT + r];
-    __syncthreads();
-    block_bitonic_sort<K, THREADS, IPT>(x, smem);
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) smem[threadIdx.x * IPT + r] = x[r];
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < n; i += THREADS) out.store(i, smem[i]);
+    K* s = reinterpret_cast<K*>(smem_raw);
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) s[pidx(i)] = in.load(i);
+    block_merge_sort<K, THREADS, EPT>(s, n);
+    for (uint32_t i = threadIdx.x; i < n; i += THREADS) out.store(i, s[pidx(i)]);
 }
 
 }  // namespace s512
