@@ -48,7 +48,7 @@ __device__ __forceinline__ void lane_stage(K (&x)[IPT], int lm) {
 #pragma unroll
     for (int r = 0; r < IPT; ++r) {
         const K y = shfl_xor(x[r], lm);
-        x[r] = upper ? kmax(x[r], y) : kmin(x[r], y);
+        x[r] = keep_side(x[r], y, upper);
     }
 }
 
@@ -62,12 +62,12 @@ __device__ __forceinline__ void lane_mirror(K (&x)[IPT], int lm, int hb) {
         const int q = IPT - 1 - r;
         const K yr = shfl_xor(x[q], lm);
         const K yq = shfl_xor(x[r], lm);
-        x[r] = upper ? kmax(x[r], yr) : kmin(x[r], yr);
-        x[q] = upper ? kmax(x[q], yq) : kmin(x[q], yq);
+        x[r] = keep_side(x[r], yr, upper);
+        x[q] = keep_side(x[q], yq, upper);
     }
     if (IPT == 1) {
         const K y = shfl_xor(x[0], lm);
-        x[0] = upper ? kmax(x[0], y) : kmin(x[0], y);
+        x[0] = keep_side(x[0], y, upper);
     }
 }
 
@@ -108,7 +108,7 @@ __device__ __forceinline__ void smem_stage(K (&x)[IPT], K* smem, unsigned m, uns
     for (int r = 0; r < IPT; ++r) {
         const unsigned e = base + r;
         const K y = smem[e ^ m];
-        x[r] = (e & hb) ? kmax(x[r], y) : kmin(x[r], y);
+        x[r] = keep_side(x[r], y, (e & hb) != 0);
     }
     __syncthreads();
 }

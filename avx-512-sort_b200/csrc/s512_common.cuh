@@ -66,37 +66,64 @@ __device__ __forceinline__ uint64_t enc_kv(int key, int val) {
 //   store(i, k)  -> write encoded key k as element i of the destination
 // `Raw` is the identity codec used on the library's own scratch buffers.
 
+// Besides load/store, every input codec describes its raw arrays (NARR
+// arrays of ESZ-byte elements, arr(k)) and decodes element i of a tile that a
+// bulk copy placed in shared memory (array k of the tile at buf + k*tile*ESZ).
 template <typename K>
 struct Raw {
     using Key = K;
+    static constexpr int NARR = 1;
+    static constexpr int ESZ = sizeof(K);
     const K* __restrict__ in;
     K* __restrict__ out;
     __device__ __forceinline__ K load(size_t i) const { return __ldg(in + i); }
     __device__ __forceinline__ void store(size_t i, K k) const { out[i] = k; }
+    __host__ __device__ const void* arr(int) const { return in; }
+    __device__ __forceinline__ K decode(const unsigned char* buf, uint32_t i, uint32_t) const {
+        return reinterpret_cast<const K*>(buf)[i];
+    }
 };
 
 struct CodecI32 {
     using Key = uint32_t;
+    static constexpr int NARR = 1;
+    static constexpr int ESZ = 4;
     const int* __restrict__ in;
     int* __restrict__ out;
     __device__ __forceinline__ uint32_t load(size_t i) const { return enc_i32(__ldg(in + i)); }
     __device__ __forceinline__ void store(size_t i, uint32_t k) const { out[i] = dec_i32(k); }
+    __host__ __device__ const void* arr(int) const { return in; }
+    __device__ __forceinline__ uint32_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
+        return enc_i32(reinterpret_cast<const int*>(buf)[i]);
+    }
 };
 
 struct CodecF64 {
     using Key = uint64_t;
+    static constexpr int NARR = 1;
+    static constexpr int ESZ = 8;
     const unsigned long long* __restrict__ in;
     unsigned long long* __restrict__ out;
     __device__ __forceinline__ uint64_t load(size_t i) const { return enc_f64_bits(__ldg(in + i)); }
     __device__ __forceinline__ void store(size_t i, uint64_t k) const { out[i] = dec_f64_bits(k); }
+    __host__ __device__ const void* arr(int) const { return in; }
+    __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
+        return enc_f64_bits(reinterpret_cast<const unsigned long long*>(buf)[i]);
+    }
 };
 
 struct CodecKV {
     using Key = uint64_t;
+    static constexpr int NARR = 2;
+    static constexpr int ESZ = 4;
     const int* __restrict__ kin;
     const int* __restrict__ vin;
     int* __restrict__ kout;
     int* __restrict__ vout;
+    __host__ __device__ const void* arr(int k) const { return k ? (const void*)vin : (const void*)kin; }
+    __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t tile) const {
+        return enc_kv(reinterpret_cast<const int*>(buf)[i], reinterpret_cast<const int*>(buf + (size_t)tile * 4)[i]);
+    }
     __device__ __forceinline__ uint64_t load(size_t i) const { return enc_kv(__ldg(kin + i), __ldg(vin + i)); }
     __device__ __forceinline__ void store(size_t i, uint64_t k) const {
         kout[i] = dec_i32((uint32_t)(k >> 32));
@@ -133,24 +160,80 @@ __device__ __forceinline__ T kmin(T a, T b) { return a < b ? a : b; }
 template <typename T>
 __device__ __forceinline__ T kmax(T a, T b) { return a < b ? b : a; }
 
-// compare-exchange: a <- min, b <- max
+// compare-exchange: a <- min, b <- max (one comparison, two selects)
 template <typename T>
 __device__ __forceinline__ void cas(T& a, T& b) {
-    T lo = kmin(a, b), hi = kmax(a, b);
+    const bool sw = b < a;
+    const T lo = sw ? b : a;
+    const T hi = sw ? a : b;
     a = lo;
     b = hi;
 }
 
+// One side of a comparator whose other key y lives in another lane: the lower
+// side keeps the minimum, the upper side the maximum.
+template <typename T>
+__device__ __forceinline__ T keep_side(T x, T y, bool upper) {
+    return ((y < x) != upper) ? y : x;
+}
+
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
-// 64-bit device-scope acquire / release for the lookback status words
-__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+// 64-bit device-scope loads / stores of look-back status words.  A status
+// word carries its flag and its count together, and nothing else is read
+// through it, so relaxed atomics suffice; acquire loads would also serialise
+// the look-back window's loads behind one another.
+__device__ __forceinline__ unsigned long long ld_status(const unsigned long long* p) {
     cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*const_cast<unsigned long long*>(p));
-    return r.load(cuda::memory_order_acquire);
+    return r.load(cuda::memory_order_relaxed);
 }
-__device__ __forceinline__ void st_release(unsigned long long* p, unsigned long long v) {
+__device__ __forceinline__ void st_status(unsigned long long* p, unsigned long long v) {
     cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> r(*p);
-    r.store(v, cuda::memory_order_release);
+    r.store(v, cuda::memory_order_relaxed);
+}
+
+// ---------------------------------------------------------------------------
+// 1-D bulk copies (TMA, no multicast) completing on a CTA mbarrier
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// order earlier generic-proxy accesses of shared memory before later
+// async-proxy (bulk copy) writes to it
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// dst, src 16-byte aligned; bytes a positive multiple of 16
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for a phase of an mbarrier; false if the limit was reached
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
+    for (uint32_t i = 0; i < SPIN_LIMIT; ++i)
+        if (mbar_try_wait(bar, phase)) return true;
+    return false;
 }
 
 // splitmix64 finaliser: counter-based hashing for sample positions

@@ -81,15 +81,15 @@ __global__ void __launch_bounds__(THREADS) partition2_kernel(const T* __restrict
             unsigned long long* st = status + (size_t)t * 2 + tid;
             uint64_t prefix = 0;
             if (t == 0) {
-                st_release(st, ST_INC_P2 | mine);
+                st_status(st, ST_INC_P2 | mine);
             } else {
-                st_release(st, ST_AGG_P2 | mine);
+                st_status(st, ST_AGG_P2 | mine);
                 uint32_t p = t - 1;
                 while (true) {
                     unsigned long long w;
                     uint32_t spins = 0;
                     while (true) {
-                        w = ld_acquire(status + (size_t)p * 2 + tid);
+                        w = ld_status(status + (size_t)p * 2 + tid);
                         if (w & (ST_INC_P2 | ST_AGG_P2)) break;
                         if (++spins > SPIN_LIMIT) break;
                         __nanosleep(spins < 64 ? 20 : 200);
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(THREADS) partition2_kernel(const T* __restrict
                     if (w & ST_INC_P2) break;
                     --p;
                 }
-                if (prefix != ~0ull) st_release(st, ST_INC_P2 | (prefix + mine));
+                if (prefix != ~0ull) st_status(st, ST_INC_P2 | (prefix + mine));
             }
             pre[tid] = prefix;
             if (t == ntiles - 1 && tid == 0 && prefix != ~0ull) ctl->total_low = prefix + mine;

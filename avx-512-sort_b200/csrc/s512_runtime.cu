@@ -89,6 +89,10 @@ cudaError_t DevCtx::prepare(const void* fn, size_t smem) {
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
+        // prefer the largest shared-memory carveout so that several such
+        // blocks can be resident on one SM
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e != cudaSuccess) return e;
     }
     smem_set[fn] = smem;
     occ.erase(fn);

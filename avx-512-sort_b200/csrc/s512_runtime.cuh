@@ -13,7 +13,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sort512cuda.h"
+#include "sort512cuda.h"
 
 namespace s512 {
 

@@ -95,6 +95,15 @@ static int sort_one_leaf(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaSt
     }
 }
 
+// The partition kernel fetches tiles by bulk copy when every input array is
+// 16-byte aligned (segment and tile offsets keep that alignment).
+template <typename C>
+static bool codec_aligned(const C& c) {
+    for (int k = 0; k < C::NARR; ++k)
+        if (reinterpret_cast<uintptr_t>(c.arr(k)) & 15u) return false;
+    return true;
+}
+
 // ---------------------------------------------------------------------------
 // One partition level: sample -> sort sample -> splitters -> partition -> plan.
 template <typename K, typename InCodec>
@@ -132,12 +141,14 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         if (!base) return S512_ERR_ALLOC;
         for (int c = 0; c <= NCLASS; ++c) items[c] = (LeafItem<K>*)(base + (size_t)c * item_cap * sizeof(LeafItem<K>));
     }
-    if (!samples || !splits || !counts || !status) return S512_ERR_ALLOC;
+    uint32_t* chain = (uint32_t*)C.get("chain", (size_t)nsegs * sizeof(uint32_t));
+    if (!samples || !splits || !counts || !status || !chain) return S512_ERR_ALLOC;
 
     const int t0 = tm.mark();
     S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
     S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
     S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
+    S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
     const uint64_t seed = config().seed + 0x9E3779B97F4A7C15ull * (uint64_t)(level + 1);
     sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed, KB);
     S512_LAUNCH_CHECK();
@@ -163,6 +174,9 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     pa.ctl = ctl;
     pa.ntiles = L.ntiles_host;
     pa.ntiles_dev = L.ntiles_dev;
+    pa.nsegs = nsegs;
+    pa.tma = codec_aligned(L.in) ? 1 : 0;
+    pa.chain = chain;
     auto pfn = partition_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
     const size_t psmem = sizeof(PartSmem<K, Shape::THREADS, Shape::IPT>);
     int pgrid = 0;
@@ -205,6 +219,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
         S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
         S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
+        S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
         pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
         S512_LAUNCH_CHECK();
         plan_kernel<K><<<nsegs, NB, 0, st>>>(pl, nsegs);

@@ -304,10 +304,27 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
 
 // ===========================================================================
 // 4. The partition pass (persistent; tiles claimed in order)
+//
+// Two-stage pipeline per block: while tile i is classified, ranked and
+// scattered, tile i+1 is already on its way into the other shared-memory
+// buffer through a 1-D bulk copy (TMA) that completes on an mbarrier.  Data
+// tiles are claimed two ahead with an atomic counter.  The position of a tile
+// in its segment's look-back chain is taken separately, from a per-segment
+// counter, when the block *starts* processing it: every earlier position then
+// belongs to a tile already being processed, so no tile waits for one that is
+// still only being fetched.  (A bucket's keys land in chain order, not input
+// order; a partition pass does not need to be stable.)  The buffer that held
+// tile i's raw keys is reused to stage its keys in bucket order for the
+// coalesced write.  When an input array is not 16-byte aligned the tiles are
+// read with plain loads instead (a.tma == 0).
+
+constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
+constexpr int LOOKBACK_W = 8;  // predecessor statuses read per look-back step
 
 template <typename K>
 struct PartArgs {
     const SegDesc* segs;
+    uint32_t nsegs;               // segment count (host-known)
     const uint32_t* tile_seg;     // global tile -> segment (nullptr: single segment 0)
     const SplitSet<K>* splits;
     K* out;                       // level output buffer
@@ -316,12 +333,15 @@ struct PartArgs {
     LevelCtl* ctl;
     uint32_t ntiles;              // used when ntiles_dev is null
     const uint32_t* ntiles_dev;   // tile count written by prepare_level_kernel
+    int tma;                      // tiles arrive by bulk copy
+    uint32_t* chain;              // per segment: look-back positions handed out so far (zeroed)
 };
 
 template <typename K, int THREADS, int IPT>
 struct PartSmem {
-    K keys[THREADS * IPT];
-    uint8_t bkt[THREADS * IPT];
+    static constexpr int TILE = THREADS * IPT;
+    alignas(128) unsigned char buf[2][TILE * sizeof(K)];
+    uint8_t bkt[TILE];
     K tree[NB];
     K uniq[NB];
     uint64_t region_off[NB];
@@ -329,42 +349,103 @@ struct PartSmem {
     uint64_t gdelta[NB];
     uint32_t hist[NB];
     uint32_t loc[NB];
+    uint32_t seg_tile_start[SEG_SMEM];
     uint32_t wtot[8];
     uint8_t range_b[NB];
     uint8_t eq_b[NB];
-    uint32_t eq_mask[NB / 32];
     uint8_t ovf[NB];
-    uint32_t tile, seg, has_eq, nbk;
+    uint32_t eq_mask[NB / 32];
+    uint64_t mbar[2];
+    uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos;
 };
 
 template <typename K, typename InCodec, int THREADS, int IPT>
-__global__ void __launch_bounds__(THREADS) partition_kernel(PartArgs<K> a, InCodec in) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, InCodec in) {
+    extern __shared__ __align__(128) unsigned char smem_part[];
     using SM = PartSmem<K, THREADS, IPT>;
-    SM& sm = *reinterpret_cast<SM*>(smem_raw);
+    SM& sm = *reinterpret_cast<SM*>(smem_part);
     constexpr int TILE = THREADS * IPT;
+    constexpr int ESZ = InCodec::ESZ;
+    constexpr int NARR = InCodec::NARR;
     const int tid = threadIdx.x;
-    uint32_t cached_seg = 0xFFFFFFFFu;
     const uint32_t ntiles = a.ntiles_dev ? *a.ntiles_dev : a.ntiles;
+    const bool small_tab = a.tile_seg && a.nsegs <= (uint32_t)SEG_SMEM;
+    uint32_t cached_seg = 0xFFFFFFFFu;
 
+    if (tid == 0) {
+        mbar_init(&sm.mbar[0], 1);
+        mbar_init(&sm.mbar[1], 1);
+        fence_mbar_init();
+        sm.abort = 0;
+    }
     for (int b = tid; b < NB; b += THREADS) sm.hist[b] = 0;
+    if (small_tab)
+        for (uint32_t i = tid; i < a.nsegs; i += THREADS) sm.seg_tile_start[i] = a.segs[i].tile_start;
+    __syncthreads();
+
+    auto seg_of = [&](uint32_t t) -> uint32_t {
+        if (!a.tile_seg) return 0u;
+        if (!small_tab) return a.tile_seg[t];
+        uint32_t lo = 0, hi = a.nsegs;  // last segment whose tile_start <= t
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (sm.seg_tile_start[mid] <= t) lo = mid; else hi = mid;
+        }
+        return lo;
+    };
+    // thread 0: start the bulk copy of tile t into buffer b
+    auto issue = [&](uint32_t t, int b) {
+        const uint32_t seg = seg_of(t);
+        const SegDesc sd = a.segs[seg];
+        const uint32_t ti = t - sd.tile_start;
+        const uint64_t first = sd.in_off + (uint64_t)ti * TILE;
+        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const uint32_t bytes = (cnt * ESZ) & ~15u;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&sm.mbar[b], bytes * NARR);
+        if (bytes) {
+#pragma unroll
+            for (int k = 0; k < NARR; ++k)
+                bulk_g2s(sm.buf[b] + (size_t)k * TILE * ESZ,
+                         static_cast<const unsigned char*>(in.arr(k)) + first * ESZ, bytes, &sm.mbar[b]);
+        }
+    };
+
+    uint32_t claim_after = 0;  // thread 0: the tile claimed for two iterations ahead
+    if (tid == 0) {
+        const uint32_t t0 = atomicAdd(&a.ctl->tile_counter, 1u);
+        const uint32_t t1 = atomicAdd(&a.ctl->tile_counter, 1u);
+        sm.tile_cur = t0;
+        sm.tile_next = t1;
+        if (a.tma && t0 < ntiles) issue(t0, 0);
+    }
+    __syncthreads();
+    uint32_t phase[2] = {0u, 0u};
+    int b = 0;
 
     while (true) {
-        if (tid == 0) sm.tile = atomicAdd(&a.ctl->tile_counter, 1u);
-        __syncthreads();
-        const uint32_t t = sm.tile;
-        if (t >= ntiles) break;
-        const uint32_t seg = a.tile_seg ? a.tile_seg[t] : 0u;
+        const uint32_t t = sm.tile_cur;
+        const uint32_t tn = sm.tile_next;
+        if (t >= ntiles || sm.abort) break;
+        __syncthreads();  // everyone has read tile_cur / tile_next
+        const uint32_t seg = seg_of(t);
+        uint32_t my_pos = 0;  // thread 0: look-back position of tile t (stored before the rank barrier)
+        if (tid == 0) {
+            if (a.tma && tn < ntiles) issue(tn, b ^ 1);
+            claim_after = atomicAdd(&a.ctl->tile_counter, 1u);  // consumed at the end of the iteration
+            my_pos = atomicAdd(&a.chain[seg], 1u);
+        }
         const SegDesc sd = a.segs[seg];
         if (seg != cached_seg) {
             const SplitSet<K>& ss = a.splits[seg];
-            for (int b = tid; b < NB; b += THREADS) {
-                sm.tree[b] = ss.tree[b];
-                sm.uniq[b] = ss.uniq[b];
-                sm.region_off[b] = ss.region_off[b];
-                sm.region_cap[b] = ss.region_cap[b];
-                sm.range_b[b] = ss.range_b[b];
-                sm.eq_b[b] = ss.eq_b[b];
+            for (int i = tid; i < NB; i += THREADS) {
+                sm.tree[i] = ss.tree[i];
+                sm.uniq[i] = ss.uniq[i];
+                sm.region_off[i] = ss.region_off[i];
+                sm.region_cap[i] = ss.region_cap[i];
+                sm.range_b[i] = ss.range_b[i];
+                sm.eq_b[i] = ss.eq_b[i];
             }
             if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
             if (tid == 0) {
@@ -373,32 +454,47 @@ __global__ void __launch_bounds__(THREADS) partition_kernel(PartArgs<K> a, InCod
             }
             cached_seg = seg;
         }
-        __syncthreads();
         const uint32_t ti = t - sd.tile_start;
         const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
         const uint64_t rem = sd.count - (uint64_t)ti * TILE;
         const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
+        bool data_ok = true;
+        if (a.tma) {
+            data_ok = mbar_wait_bounded(&sm.mbar[b], phase[b]);
+            phase[b] ^= 1u;
+            if (!data_ok) raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
+        }
+        __syncthreads();  // split set in shared memory
         const bool has_eq = sm.has_eq != 0;
 
-        // load (striped: element r*THREADS + tid) and classify
+        // keys: striped element r*THREADS + tid, from the bulk-copied tile
+        // (tail elements past the copied bytes from global memory)
         K key[IPT];
         uint32_t br[IPT];  // bucket | rank << 8
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
-            if (idx < cnt) key[r] = in.load(base + idx);
+            if (idx < cnt) key[r] = idx < tma_elems ? in.decode(sm.buf[b], idx, TILE) : in.load(base + idx);
+        }
+        // all IPT tree searches first: they are independent chains of shared
+        // loads, so the scheduler can overlap them
+        uint32_t bks[IPT];
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t idx = (uint32_t)(r * THREADS + tid);
+            // lanes past the end of the tile carry the out-of-range bucket NB
+            bks[r] = idx < cnt ? find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask)
+                               : (uint32_t)NB;
         }
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
             const bool valid = idx < cnt;
-            // every lane takes part in the warp votes below; lanes past the end
-            // of the tile carry the out-of-range bucket NB
-            const uint32_t b = valid ? find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask)
-                                     : (uint32_t)NB;
+            const uint32_t bk = bks[r];
             // warp-uniform bucket (sorted / few-distinct input): one atomic for the warp
-            const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, b, 0);
-            const bool uni = __all_sync(0xFFFFFFFFu, b == b0);
+            const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, bk, 0);
+            const bool uni = __all_sync(0xFFFFFFFFu, bk == b0);
             uint32_t rank = 0;
             if (uni) {
                 if (b0 < (uint32_t)NB) {
@@ -407,78 +503,119 @@ __global__ void __launch_bounds__(THREADS) partition_kernel(PartArgs<K> a, InCod
                     rank = __shfl_sync(0xFFFFFFFFu, basev, 0) + lane_id();
                 }
             } else if (valid) {
-                rank = atomicAdd(&sm.hist[b], 1u);
+                rank = atomicAdd(&sm.hist[bk], 1u);
             }
-            br[r] = b | (rank << 8);
+            br[r] = bk | (rank << 8);
         }
+        if (tid == 0) sm.pos = my_pos;
         __syncthreads();
 
-        // publish this tile's aggregate (or its inclusive prefix if first in segment)
+        // publish this tile's aggregate (or its inclusive count if first in chain)
+        const uint32_t pos = sm.pos;
+        const uint32_t slot = sd.tile_start + pos;
         uint32_t h = 0;
         if (tid < NB) {
             h = sm.hist[tid];
-            const unsigned long long w = (ti == 0 ? ST_INC : ST_AGG) | (unsigned long long)h;
-            st_release(&a.status[(size_t)t * NB + tid], w);
+            const unsigned long long w = (pos == 0 ? ST_INC : ST_AGG) | (unsigned long long)h;
+            st_status(&a.status[(size_t)slot * NB + tid], w);
         }
-        const uint32_t excl = block_exclusive_scan_first<NB, uint32_t>(h, sm.wtot, (uint32_t*)nullptr);
-        if (tid < NB) sm.loc[tid] = excl;
+        // exclusive scan of the 256 bucket counts by warp 0 (8 per lane)
+        if (tid < 32) {
+            uint32_t v[NB / 32];
+            uint32_t run = 0;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) {
+                v[i] = run;
+                run += sm.hist[tid * (NB / 32) + i];
+            }
+            uint32_t inc = run;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+                if (tid >= d) inc += o;
+            }
+            const uint32_t ex = inc - run;
+#pragma unroll
+            for (int i = 0; i < NB / 32; ++i) sm.loc[tid * (NB / 32) + i] = ex + v[i];
+        }
         __syncthreads();
 
-        // stage keys into shared memory in bucket order
+        // stage keys in bucket order, reusing this tile's buffer
+        K* stage = reinterpret_cast<K*>(sm.buf[b]);
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
             if (idx < cnt) {
-                const uint32_t b = br[r] & 0xFFu;
-                const uint32_t p = sm.loc[b] + (br[r] >> 8);
-                sm.keys[p] = key[r];
-                sm.bkt[p] = (uint8_t)b;
+                const uint32_t bk = br[r] & 0xFFu;
+                const uint32_t p = sm.loc[bk] + (br[r] >> 8);
+                stage[p] = key[r];
+                sm.bkt[p] = (uint8_t)bk;
             }
         }
 
         // decoupled look-back: one thread per bucket
         if (tid < NB) {
             uint64_t prefix = 0;
-            bool ok = true;
-            if (ti > 0) {
-                uint32_t p = t - 1;
-                while (true) {
-                    unsigned long long v;
-                    uint32_t spins = 0;
-                    while (true) {
-                        v = ld_acquire(&a.status[(size_t)p * NB + tid]);
-                        if (v & (ST_INC | ST_AGG)) break;
-                        if (++spins > SPIN_LIMIT) break;
-                        __nanosleep(spins < 64 ? 20 : 200);
+            bool ok = data_ok;
+            if (pos > 0) {
+                // walk back through the chain LOOKBACK_W slots at a time (the
+                // loads of one window are in flight together); the segment's
+                // first slot always holds an inclusive count, so the walk ends
+                constexpr int W = LOOKBACK_W;
+                int64_t p = (int64_t)slot - 1;
+                const int64_t first = (int64_t)sd.tile_start;
+                bool done = false;
+                while (!done && ok) {
+                    unsigned long long v[W];
+#pragma unroll
+                    for (int w = 0; w < W; ++w)
+                        v[w] = (p - w >= first) ? ld_status(&a.status[(size_t)(p - w) * NB + tid]) : 0ull;
+#pragma unroll
+                    for (int w = 0; w < W; ++w) {
+                        if (done || !ok || p - w < first) continue;
+                        uint32_t spins = 0;
+                        while (!(v[w] & (ST_INC | ST_AGG))) {
+                            if (++spins > SPIN_LIMIT) break;
+                            __nanosleep(spins < 64 ? 20 : 200);
+                            v[w] = ld_status(&a.status[(size_t)(p - w) * NB + tid]);
+                        }
+                        if (!(v[w] & (ST_INC | ST_AGG))) {
+                            ok = false;
+                            raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
+                            continue;
+                        }
+                        prefix += v[w] & ST_VAL;
+                        if (v[w] & ST_INC) done = true;
                     }
-                    if (!(v & (ST_INC | ST_AGG))) {
-                        ok = false;
-                        raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
-                        break;
-                    }
-                    prefix += v & ST_VAL;
-                    if (v & ST_INC) break;
-                    --p;
+                    p -= W;
                 }
-                st_release(&a.status[(size_t)t * NB + tid], ST_INC | (unsigned long long)(prefix + h));
+                st_status(&a.status[(size_t)slot * NB + tid], ST_INC | (unsigned long long)(prefix + h));
             }
             const uint64_t end = prefix + h;
             const bool ovf = !ok || end > sm.region_cap[tid];
             if (ovf && h) raise_error(&a.ctl->err, ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
             sm.ovf[tid] = ovf ? 1 : 0;
             sm.gdelta[tid] = sd.out_base + sm.region_off[tid] + prefix - (uint64_t)sm.loc[tid];
-            if (ti == sd.ntiles - 1) a.bucket_counts[(size_t)seg * NB + tid] = end;
+            if (pos == sd.ntiles - 1) a.bucket_counts[(size_t)seg * NB + tid] = end;
         }
         __syncthreads();
 
         // coalesced write-out
         for (uint32_t i = tid; i < cnt; i += THREADS) {
-            const uint32_t b = sm.bkt[i];
-            if (!sm.ovf[b]) a.out[sm.gdelta[b] + i] = sm.keys[i];
+            const uint32_t bk = sm.bkt[i];
+            if (!sm.ovf[bk]) a.out[sm.gdelta[bk] + i] = stage[i];
         }
         if (tid < NB) sm.hist[tid] = 0;
+        if (tid == 0) {
+            sm.tile_cur = tn;
+            sm.tile_next = claim_after;
+            if (!data_ok) sm.abort = 1;
+        }
         __syncthreads();
+        b ^= 1;
     }
+    // after an abort, let a copy still in flight land before the block exits
+    if (a.tma && sm.abort && tid == 0 && sm.tile_cur < ntiles) mbar_wait_bounded(&sm.mbar[b], phase[b]);
 }
 
 // Exact histogram of a level (the fallback after a capacity overflow).

@@ -328,3 +328,27 @@ def test_stats_are_reported(s512, cuda):
         assert st["fallbacks"] == 0
     finally:
         s512.set_config(collect_stats=0)
+
+
+def test_unaligned_device_input(s512, cuda, oracle):
+    # a sub-array that starts 1 element into an allocation is not 16-byte
+    # aligned: the partition pass reads it with plain loads instead of bulk copies
+    import torch
+    import workloads
+    for dt, n in ((torch.int32, 300001), (torch.float64, 200003)):
+        base = (workloads.uniform_i32_torch(n + 1, 21) if dt == torch.int32
+                else workloads.uniform01_torch(n + 1, 21)).to(cuda)
+        t = base[1:]
+        assert t.data_ptr() % 16 != 0
+        ref = torch.sort(t.clone()).values
+        s512.sort(t)
+        assert torch.equal(t, ref)
+        assert base[0].item() == (workloads.uniform_i32_torch(1, 21) if dt == torch.int32
+                                  else workloads.uniform01_torch(1, 21)).item()
+    k = workloads.uniform_i32_torch(100001, 22)
+    v = torch.arange(100001, dtype=torch.int32, device=cuda)
+    kk, vv = k[1:].clone(), v[1:].clone()
+    k1, v1 = k[1:], v[1:]
+    s512.sort_kv(k1, v1)
+    assert torch.equal(k1, torch.sort(kk).values)
+    assert torch.equal(kk[(v1 - 1).long()], k1)
