@@ -42,6 +42,7 @@ EXPORTS = (
     "s512_smallsort_i32", "s512_smallsort_f64", "s512_smallsort_kv_i32",
     "s512_core_small_sort_i32", "s512_core_small_sort_f64", "s512_core_small_sort_kv_i32",
     "s512_popcount",
+    "s512_partition_i32_noalloc",
 )
 
 
@@ -128,6 +129,7 @@ def lib() -> ctypes.CDLL:
     L.s512_smallsort_kv_i32.argtypes = [vp, vp, sz, ci, vp]
     L.s512_core_small_sort_kv_i32.argtypes = [vp, vp, ci, ci, vp]
     L.s512_popcount.argtypes = [ctypes.c_uint]
+    L.s512_partition_i32_noalloc.argtypes = [vp, sz, sz, ctypes.c_int, szp, vp]
     _lib = L
     return L
 
@@ -232,6 +234,21 @@ def partition_kv(keys, values, left: int, right: int, pivot: int, flags: int = 0
     _check("s512_partition_kv_i32", lib().s512_partition_kv_i32(pk, pv, left, right, pivot, ctypes.byref(out),
                                                                 _flags(dev, flags), _stream(stream)))
     return out.value
+
+
+def partition_noalloc(a, left: int, right: int, pivot: int, stream=None) -> int:
+    """Partition512 on int32 device data without any allocation (fixed scratch
+    of NOALLOC_MAX_ELEMS elements)."""
+    p, n, dt, dev = _ptr(a)
+    if dt != "int32" or not dev:
+        raise ValueError("partition_noalloc takes an int32 CUDA tensor")
+    out = ctypes.c_size_t(0)
+    _check("s512_partition_i32_noalloc",
+           lib().s512_partition_i32_noalloc(p, left, right, pivot, ctypes.byref(out), _stream(stream)))
+    return out.value
+
+
+NOALLOC_MAX_ELEMS = 1 << 20
 
 
 def popcount(mask: int) -> int:

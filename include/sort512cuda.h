@@ -135,6 +135,19 @@ S512_API int s512_core_small_sort_kv_i32(int* keys, int* values, int nvec, int f
 /* --- Sort512::popcount(__mmask16)   sort512.hpp:5714-5725 */
 S512_API int s512_popcount(unsigned mask);
 
+/* --- No counterpart in the reference.  Partition512 on int32 device data for
+ *     callers that must not allocate (a framework's allocator owns all device
+ *     memory, a real-time host forbids allocations after start-up, ...):
+ *     same kernel and result as s512_partition_i32 with S512_PTR_DEVICE, but
+ *     its scratch is a fixed device array of S512_NOALLOC_MAX_ELEMS ints plus
+ *     a few KB, held by every GPU that loads the library until exit.  Larger
+ *     ranges return S512_ERR_ARG.  The first call on a device looks up that
+ *     array and should come before any stream capture; calls that overlap on
+ *     the GPU share the array and race.  Waits for the result. */
+#define S512_NOALLOC_MAX_ELEMS (1u << 20)
+S512_API int s512_partition_i32_noalloc(int* data, size_t left, size_t right, int pivot, size_t* boundary,
+                                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif
