@@ -43,6 +43,7 @@ EXPORTS = (
     "s512_core_small_sort_i32", "s512_core_small_sort_f64", "s512_core_small_sort_kv_i32",
     "s512_popcount",
     "s512_partition_i32_noalloc",
+    "s512_merge_i32", "s512_merge_f64", "s512_sort_omp_merge_i32", "s512_sort_omp_merge_f64",
 )
 
 
@@ -130,6 +131,9 @@ def lib() -> ctypes.CDLL:
     L.s512_core_small_sort_kv_i32.argtypes = [vp, vp, ci, ci, vp]
     L.s512_popcount.argtypes = [ctypes.c_uint]
     L.s512_partition_i32_noalloc.argtypes = [vp, sz, sz, ctypes.c_int, szp, vp]
+    for suf in ("i32", "f64"):
+        getattr(L, f"s512_merge_{suf}").argtypes = [vp, sz, sz, ci, vp]
+        getattr(L, f"s512_sort_omp_merge_{suf}").argtypes = [vp, sz, ci, ci, vp]
     _lib = L
     return L
 
@@ -202,6 +206,20 @@ def partition(a, left: int, right: int, pivot, flags: int = 0, stream=None) -> i
     fn = f"s512_partition_{_suffix(dt)}"
     _check(fn, getattr(lib(), fn)(p, left, right, pivot, ctypes.byref(out), _flags(dev, flags), _stream(stream)))
     return out.value
+
+
+def merge(a, middle: int, flags: int = 0, stream=None) -> None:
+    """Merge the sorted runs a[:middle] and a[middle:] in place (stable)."""
+    p, n, dt, dev = _ptr(a)
+    fn = f"s512_merge_{_suffix(dt)}"
+    _check(fn, getattr(lib(), fn)(p, n, middle, _flags(dev, flags), _stream(stream)))
+
+
+def sort_omp_merge(a, nparts: int = 8, flags: int = 0, stream=None) -> None:
+    """Sort512::SortOmpMerge / SortOmpParMerge: chunk sorts + merge-path tree."""
+    p, n, dt, dev = _ptr(a)
+    fn = f"s512_sort_omp_merge_{_suffix(dt)}"
+    _check(fn, getattr(lib(), fn)(p, n, nparts, _flags(dev, flags), _stream(stream)))
 
 
 # -- Sort512kv ----------------------------------------------------------------

@@ -132,6 +132,21 @@ S512_API int s512_core_small_sort_i32(int* data, int nvec, int flags, void* stre
 S512_API int s512_core_small_sort_f64(double* data, int nvec, int flags, void* stream);
 S512_API int s512_core_small_sort_kv_i32(int* keys, int* values, int nvec, int flags, void* stream);
 
+/* --- Merge two sorted runs in place: data[0, middle) and data[middle, n).
+ *     ParallelInplace::parallelMergeInPlace (parallelInplace.hpp:210-306) and
+ *     std::inplace_merge as called by SortOmpMerge (sort512.hpp:6045).
+ *     Stable: on equal keys the left run's element comes first. */
+S512_API int s512_merge_i32(int* data, size_t n, size_t middle, int flags, void* stream);
+S512_API int s512_merge_f64(double* data, size_t n, size_t middle, int flags, void* stream);
+
+/* --- Sort512::SortOmpMerge / SortOmpMergeDeps / SortOmpParMerge
+ *     (sort512.hpp:6006-6058, 6060-6102, 6104-6174): sort nparts chunks of
+ *     ceil(n/nparts) keys each, then merge neighbouring runs level by level
+ *     with merge-path merges.  Any nparts >= 1 (the reference needs a power
+ *     of two <= 128). */
+S512_API int s512_sort_omp_merge_i32(int* data, size_t n, int nparts, int flags, void* stream);
+S512_API int s512_sort_omp_merge_f64(double* data, size_t n, int nparts, int flags, void* stream);
+
 /* --- Sort512::popcount(__mmask16)   sort512.hpp:5714-5725 */
 S512_API int s512_popcount(unsigned mask);
 

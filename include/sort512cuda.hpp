@@ -13,6 +13,7 @@
 //   Sort512::SmallSort16V(int*|double*, size_t length)               5312/2255
 //   Sort512::CoreSmallSort, CoreSmallSort2..16 (pointer forms)
 //   Sort512::popcount(mask)                                          5714
+//   ParallelInplace::parallelMergeInPlace(array, size, center)       parallelInplace.hpp:210
 //   Sort512kv::Sort / SortOmpPartition<T,IndexType>(T keys[], T values[], IndexType size)  sort512kv.hpp:6133/6165
 //   Sort512kv::Partition512<IndexType>(int keys[], int values[], left, right, pivot)       5960
 //   Sort512kv::SmallSort16V(int*, int*, size_t)                                            5235
@@ -24,8 +25,9 @@
 // thread counts that are not powers of two) these functions are defined:
 // size 0 is a no-op and any length is sorted.  A failure of the device or of
 // an allocation throws Sort512::Error (the reference has no error path).
-// SortOmpMerge/MergeDeps/ParMerge produce the same sorted array as Sort; on
-// the GPU the OpenMP distinctions do not apply.
+// SortOmpPartition runs the partition sort; SortOmpMerge/MergeDeps/ParMerge
+// keep the reference's method (chunk sorts, then a merge tree) with
+// merge-path merges; all return the same sorted array.
 #ifndef SORT512CUDA_HPP
 #define SORT512CUDA_HPP
 
@@ -84,17 +86,32 @@ template <class SortType, class IndexType = size_t>
 inline void SortOmpPartition(SortType array[], const IndexType size) {
     Sort<SortType, IndexType>(array, size);
 }
+namespace detail {
+inline int call_merge_sort(int* a, size_t n, int parts) {
+    return s512_sort_omp_merge_i32(a, n, parts, S512_PTR_AUTO, nullptr);
+}
+inline int call_merge_sort(double* a, size_t n, int parts) {
+    return s512_sort_omp_merge_f64(a, n, parts, S512_PTR_AUTO, nullptr);
+}
+inline int call_merge(int* a, size_t n, size_t mid) { return s512_merge_i32(a, n, mid, S512_PTR_AUTO, nullptr); }
+inline int call_merge(double* a, size_t n, size_t mid) { return s512_merge_f64(a, n, mid, S512_PTR_AUTO, nullptr); }
+// chunks of the merge-based drivers: the reference uses one per OpenMP thread
+constexpr int kMergeParts = 8;
+}  // namespace detail
+
+// Chunk sorts followed by a tree of merges, as in the reference; on the GPU
+// every merge is a merge-path pass.
 template <class SortType, class IndexType = size_t>
 inline void SortOmpMerge(SortType array[], const IndexType size) {
-    Sort<SortType, IndexType>(array, size);
+    detail::check("Sort512::SortOmpMerge", detail::call_merge_sort(array, (size_t)size, detail::kMergeParts));
 }
 template <class SortType, class IndexType = size_t>
 inline void SortOmpMergeDeps(SortType array[], const IndexType size) {
-    Sort<SortType, IndexType>(array, size);
+    detail::check("Sort512::SortOmpMergeDeps", detail::call_merge_sort(array, (size_t)size, detail::kMergeParts));
 }
 template <class SortType, class IndexType = size_t>
 inline void SortOmpParMerge(SortType array[], const IndexType size) {
-    Sort<SortType, IndexType>(array, size);
+    detail::check("Sort512::SortOmpParMerge", detail::call_merge_sort(array, (size_t)size, detail::kMergeParts));
 }
 
 // The reference's README names SortOmp(); the real symbols are the four above.
@@ -209,6 +226,18 @@ S512_CORE_SMALL_SORT_OVERLOADS(double, 8)
 #undef S512_CORE_SMALL_SORT_OVERLOADS
 
 }  // namespace Sort512
+
+// ParallelInplace::parallelMergeInPlace (parallelInplace.hpp:210): merge the
+// sorted runs array[0, centerPosition) and array[centerPosition, sizeArray).
+// The OpenMP plumbing arguments of the reference (thread count, first thread,
+// interval and barrier arrays) have no meaning on the GPU and are dropped.
+namespace ParallelInplace {
+template <class NumType>
+inline void parallelMergeInPlace(NumType array[], const long sizeArray, const long centerPosition) {
+    Sort512::detail::check("ParallelInplace::parallelMergeInPlace",
+                           Sort512::detail::call_merge(array, (size_t)sizeArray, (size_t)centerPosition));
+}
+}  // namespace ParallelInplace
 
 namespace Sort512kv {
 

@@ -314,6 +314,25 @@ static void test_partition_pair() {
     for (size_t n = 1; n <= 1000; ++n) one(n);
 }
 
+// ParallelInplace::parallelMergeInPlace on two sorted halves (parallelInplace.hpp:210)
+template <class T>
+static void test_parallel_merge() {
+    std::printf("parallelMergeInPlace %s\n", sizeof(T) == 4 ? "int" : "double");
+    for (size_t n : {size_t(2), size_t(17), size_t(1000), size_t(65537), size_t(1) << 20}) {
+        for (size_t center : {size_t(1), n / 3, n / 2, n - 1}) {
+            if (center == 0 || center >= n) continue;
+            std::vector<T> a(n);
+            rand_vec(a.data(), n);
+            std::sort(a.begin(), a.begin() + center);
+            std::sort(a.begin() + center, a.end());
+            std::vector<T> want(a);
+            std::inplace_merge(want.begin(), want.begin() + center, want.end());
+            ParallelInplace::parallelMergeInPlace(a.data(), (long)n, (long)center);
+            assert_equal(a.data(), want.data(), n, "parallelMergeInPlace");
+        }
+    }
+}
+
 int main() {
     test_popcount();
     test_sort_nvec<int, 16>();
@@ -328,6 +347,8 @@ int main() {
     test_partition<int>();
     test_partition<double>();
     test_partition_pair();
+    test_parallel_merge<int>();
+    test_parallel_merge<double>();
     if (g_fail) std::printf("Test failed!\n");
     else std::printf("All tests passed\n");
     return g_fail;

@@ -352,3 +352,51 @@ def test_unaligned_device_input(s512, cuda, oracle):
     s512.sort_kv(k1, v1)
     assert torch.equal(k1, torch.sort(kk).values)
     assert torch.equal(kk[(v1 - 1).long()], k1)
+
+
+# ---- merge path (SortOmpMerge / SortOmpParMerge / parallelMergeInPlace) ----
+def test_merge_matches_restated_inplace_merge(s512, cuda, oracle):
+    import workloads
+    rng = np.random.default_rng(4)
+    for dt in (np.int32, np.float64):
+        for n, mid in ((2, 1), (10, 3), (4097, 4096), (5000, 17), (100000, 50000), (1 << 20, 123457),
+                       (1 << 20, (1 << 20) - 1), (300000, 299000)):
+            a = workloads.uniform_i32_np(n, n) if dt == np.int32 else workloads.uniform01_np(n, n)
+            if dt == np.int32:
+                a = (a % 1000).astype(np.int32)  # many ties: stability is visible
+            a[:mid].sort()
+            a[mid:].sort()
+            b = a.copy()
+            s512.merge(a, mid)
+            oracle.merge(b, mid)
+            assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (dt, n, mid)
+
+
+def test_merge_keeps_signed_zero_order(s512, cuda, oracle):
+    # -0.0 and +0.0 compare equal: a stable merge keeps the left run's zeros first
+    a = np.array([-1.0, -0.0, 0.0, 2.0, -0.5, 0.0, -0.0, 3.0])
+    b = a.copy()
+    s512.merge(a, 4)
+    oracle.merge(b, 4)
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_sort_omp_merge_matches_reference(golden, oracle, s512, cuda):
+    for case in golden["sort_omp"]:
+        if case["fn"] not in ("sort_omp_merge", "sort_omp_merge_deps", "sort_omp_parmerge"):
+            continue
+        st = oracle.rng(case["seed"])
+        a = oracle.rand_vec(st, case["n"], case["dtype"])
+        s512.sort_omp_merge(a, 8)
+        assert digest(a) == case["digest"], case
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3, 7, 8, 64])
+def test_sort_omp_merge_any_part_count(parts, s512, cuda):
+    import torch
+    import workloads
+    n = 1_000_003
+    t0 = workloads.uniform_i32_torch(n, parts)
+    t = t0.clone()
+    s512.sort_omp_merge(t, parts)
+    assert torch.equal(t, torch.sort(t0).values)
