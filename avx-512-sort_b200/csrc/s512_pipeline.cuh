@@ -1,0 +1,439 @@
+// s512_pipeline.cuh -- host driver of the partition-then-sort pipeline
+// (included by the translation units that sort: s512_sort.cu, s512_segsort.cu).
+#pragma once
+
+#include "s512_runtime.cuh"
+#include "s512_sortpipe.cuh"
+
+namespace s512 {
+
+// Tile shapes of the partition kernel per key size.
+template <typename K> struct PartShape;
+template <> struct PartShape<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
+template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT = 8; };
+
+// ---------------------------------------------------------------------------
+// leaf launches per class
+
+template <typename K, typename OutCodec, int THREADS, int EPT>
+static int launch_leaf_block(DevCtx& C, const LeafItem<K>* items, uint32_t n, OutCodec out, cudaStream_t st) {
+    auto fn = leaf_block_kernel<K, OutCodec, THREADS, EPT>;
+    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
+    int grid = 0;
+    S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
+    fn<<<grid, THREADS, smem, st>>>(items, n, out);
+    S512_LAUNCH_CHECK();
+    return S512_OK;
+}
+
+template <typename K, typename OutCodec>
+static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint32_t n, OutCodec out,
+                             cudaStream_t st) {
+    if (n == 0) return S512_OK;
+    switch (cls) {
+        case 0: {
+            auto fn = leaf_warp_kernel<K, OutCodec, 8>;
+            int grid = 0;
+            S512_CUDA_TRY(launch_persistent(C, fn, 256, 0, st, (int)((n + 7) / 8), &grid));
+            fn<<<grid, 256, 0, st>>>(items, n, out);
+            S512_LAUNCH_CHECK();
+            return S512_OK;
+        }
+        case 1: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, st);
+        case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, st);
+        case 3: return launch_leaf_block<K, OutCodec, 512, 8>(C, items, n, out, st);
+        case 4: return launch_leaf_block<K, OutCodec, 1024, 8>(C, items, n, out, st);
+        case 5: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, st);
+        case CLS_COPY: {
+            auto fn = leaf_copy_kernel<K, OutCodec>;
+            int grid = 0;
+            S512_CUDA_TRY(launch_persistent(C, fn, 256, 0, st, (int)n, &grid));
+            fn<<<grid, 256, 0, st>>>(items, n, out);
+            S512_LAUNCH_CHECK();
+            return S512_OK;
+        }
+    }
+    set_error("bad leaf class %d", cls);
+    return S512_ERR_INTERNAL;
+}
+
+// Whole array in one leaf (n <= leaf_max).
+template <typename InCodec, typename OutCodec, int THREADS, int EPT>
+static int launch_small_block(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaStream_t st) {
+    using K = typename InCodec::Key;
+    auto fn = small_block_sort_kernel<InCodec, OutCodec, THREADS, EPT>;
+    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
+    S512_CUDA_TRY(C.prepare((const void*)fn, smem));
+    fn<<<1, THREADS, smem, st>>>(in, out, n);
+    S512_LAUNCH_CHECK();
+    return S512_OK;
+}
+
+template <typename InCodec, typename OutCodec>
+static int sort_one_leaf(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaStream_t st) {
+    using K = typename InCodec::Key;
+    if (n <= 256) {
+        small_warp_sort_kernel<InCodec, OutCodec, 8><<<1, 32, 0, st>>>(in, out, n);
+        S512_LAUNCH_CHECK();
+        return S512_OK;
+    }
+    switch (class_of(sizeof(K), n)) {
+        case 1: return launch_small_block<InCodec, OutCodec, 128, 8>(C, in, out, n, st);
+        case 2: return launch_small_block<InCodec, OutCodec, 256, 8>(C, in, out, n, st);
+        case 3: return launch_small_block<InCodec, OutCodec, 512, 8>(C, in, out, n, st);
+        case 4: return launch_small_block<InCodec, OutCodec, 1024, 8>(C, in, out, n, st);
+        default: return launch_small_block<InCodec, OutCodec, 1024, 16>(C, in, out, n, st);
+    }
+}
+
+// The partition kernel fetches tiles by bulk copy when every input array is
+// 16-byte aligned (segment and tile offsets keep that alignment).
+template <typename C>
+static bool codec_aligned(const C& c) {
+    for (int k = 0; k < C::NARR; ++k)
+        if (reinterpret_cast<uintptr_t>(c.arr(k)) & 15u) return false;
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// One partition level: sample -> sort sample -> splitters -> partition -> plan.
+template <typename K, typename InCodec>
+struct Level {
+    InCodec in;
+    SegDesc* segs;
+    uint32_t nsegs;
+    const uint32_t* tile_seg;   // null for a single segment
+    uint32_t ntiles_host;       // level 0
+    const uint32_t* ntiles_dev; // levels >= 1
+    uint32_t ntiles_bound;
+    K* out;
+    bool aligned;               // every tile starts 16-byte aligned (bulk copies allowed)
+};
+
+template <typename K, typename InCodec, typename UserOut>
+static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, size_t n, cudaStream_t st,
+                     LevelCtl* ctl, LevelCtl* next_ctl_dev, SegDesc* next_segs, uint32_t next_cap,
+                     PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl) {
+    constexpr int KB = sizeof(K);
+    using Shape = PartShape<K>;
+    constexpr int TILE = Shape::THREADS * Shape::IPT;
+    const uint32_t nsegs = L.nsegs;
+    int rc;
+
+    // scratch for this level
+    K* samples = (K*)C.get("samples", (size_t)nsegs * SAMPLE_N * KB);
+    SplitSet<K>* splits = (SplitSet<K>*)C.get("splits", (size_t)nsegs * sizeof(SplitSet<K>));
+    uint64_t* counts = (uint64_t*)C.get("counts", (size_t)nsegs * NB * sizeof(uint64_t));
+    unsigned long long* status =
+        (unsigned long long*)C.get("status", (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long));
+    const uint32_t item_cap = nsegs * NB + (uint32_t)(n / COPY_CHUNK) + 16;
+    LeafItem<K>* items[NCLASS + 1];
+    {
+        char* base = (char*)C.get("items", (size_t)(NCLASS + 1) * item_cap * sizeof(LeafItem<K>));
+        if (!base) return S512_ERR_ALLOC;
+        for (int c = 0; c <= NCLASS; ++c) items[c] = (LeafItem<K>*)(base + (size_t)c * item_cap * sizeof(LeafItem<K>));
+    }
+    uint32_t* chain = (uint32_t*)C.get("chain", (size_t)nsegs * sizeof(uint32_t));
+    if (!samples || !splits || !counts || !status || !chain) return S512_ERR_ALLOC;
+
+    const int t0 = tm.mark();
+    S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
+    S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
+    S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
+    S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
+    const uint64_t seed = config().seed + 0x9E3779B97F4A7C15ull * (uint64_t)(level + 1);
+    sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed, KB);
+    S512_LAUNCH_CHECK();
+    {
+        auto fn = sample_sort_kernel<K>;
+        const size_t smem = (size_t)padded_len(SAMPLE_N) * KB;
+        S512_CUDA_TRY(C.prepare((const void*)fn, smem));
+        fn<<<nsegs, 1024, smem, st>>>(samples, L.segs, nsegs, KB);
+        S512_LAUNCH_CHECK();
+    }
+    splitter_kernel<K><<<nsegs, NB, 0, st>>>(samples, L.segs, nsegs, splits, KB);
+    S512_LAUNCH_CHECK();
+    S.kernel_launches += 3;
+    const int t1 = tm.mark();
+
+    PartArgs<K> pa;
+    pa.segs = L.segs;
+    pa.tile_seg = L.tile_seg;
+    pa.splits = splits;
+    pa.out = L.out;
+    pa.status = status;
+    pa.bucket_counts = counts;
+    pa.ctl = ctl;
+    pa.ntiles = L.ntiles_host;
+    pa.ntiles_dev = L.ntiles_dev;
+    pa.nsegs = nsegs;
+    pa.tma = (L.aligned && codec_aligned(L.in)) ? 1 : 0;
+    pa.chain = chain;
+    auto pfn = partition_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
+    const size_t psmem = sizeof(PartSmem<K, Shape::THREADS, Shape::IPT>);
+    int pgrid = 0;
+    S512_CUDA_TRY(launch_persistent(C, pfn, Shape::THREADS, psmem, st, 0, &pgrid));
+    pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
+    S512_LAUNCH_CHECK();
+    S.kernel_launches += 1;
+    const int t2 = tm.mark();
+
+    PlanArgs<K> pl;
+    pl.segs = L.segs;
+    pl.splits = splits;
+    pl.bucket_counts = counts;
+    pl.level_out = L.out;
+    for (int c = 0; c <= NCLASS; ++c) pl.items[c] = items[c];
+    pl.item_cap = item_cap;
+    pl.next = next_segs;
+    pl.next_cap = next_cap;
+    pl.ctl = ctl;
+    pl.key_bytes = KB;
+    plan_kernel<K><<<nsegs, NB, 0, st>>>(pl, nsegs);
+    S512_LAUNCH_CHECK();
+    S512_CUDA_TRY(cudaMemcpyAsync(host_ctl, ctl, sizeof(LevelCtl), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaStreamSynchronize(st));
+    S.kernel_launches += 1;
+
+    if (host_ctl->err & DEV_ERR_OVERFLOW) {
+        // a bucket outgrew its sampled capacity: exact counts, exact regions, redo
+        S.fallbacks += 1;
+        const uint32_t ntiles = L.ntiles_dev ? host_ctl->ntiles_next : L.ntiles_host;
+        (void)ntiles;
+        S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
+        auto cfn = count_kernel<K, InCodec, 256, Shape::IPT>;
+        int cgrid = 0;
+        S512_CUDA_TRY(launch_persistent(C, cfn, 256, 0, st, 0, &cgrid));
+        cfn<<<cgrid, 256, 0, st>>>(pa, L.in);
+        S512_LAUNCH_CHECK();
+        exact_regions_kernel<K><<<nsegs, NB, 0, st>>>(splits, counts, nsegs);
+        S512_LAUNCH_CHECK();
+        S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
+        S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
+        S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
+        S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
+        pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
+        S512_LAUNCH_CHECK();
+        plan_kernel<K><<<nsegs, NB, 0, st>>>(pl, nsegs);
+        S512_LAUNCH_CHECK();
+        S512_CUDA_TRY(cudaMemcpyAsync(host_ctl, ctl, sizeof(LevelCtl), cudaMemcpyDeviceToHost, st));
+        S512_CUDA_TRY(cudaStreamSynchronize(st));
+        S.kernel_launches += 5;
+    }
+    if (host_ctl->err) {
+        if (host_ctl->err & DEV_ERR_TIMEOUT) {
+            set_error("partition look-back wait timed out at level %d", level);
+            return S512_ERR_TIMEOUT;
+        }
+        set_error("partition level %d reported device error 0x%x", level, host_ctl->err);
+        return S512_ERR_INTERNAL;
+    }
+
+    // leaves of this level
+    const int t3 = tm.mark();
+    for (int c = 0; c <= NCLASS; ++c) {
+        if (host_ctl->n_items[c] == 0) continue;
+        rc = launch_leaf_class<K, UserOut>(C, c, items[c], host_ctl->n_items[c], uout, st);
+        if (rc) return rc;
+        S.kernel_launches += 1;
+    }
+    const int t4 = tm.mark();
+
+    if (level < S512_MAX_LEVELS) {
+        S.partition_keys[level] += (level == 0) ? (uint64_t)n : 0;
+        S.partition_launches[level] += 1;
+        if (tm.on()) {
+            S.sample_ms[level] += tm.ms(t0, t1);
+            S.partition_ms[level] += tm.ms(t1, t2);
+            S.leaf_ms[level] += tm.ms(t2, t4);
+        }
+        (void)t3;
+        // imbalance: largest bucket over the mean non-empty bucket of the level
+        if (host_ctl->nonempty && host_ctl->level_keys)
+            S.max_bucket_over_mean[level] =
+                (double)host_ctl->max_bucket / ((double)host_ctl->level_keys / (double)host_ctl->nonempty);
+    }
+    (void)next_ctl_dev;
+    return S512_OK;
+}
+
+// Partition levels starting from `nsegs0` segments of the caller's array
+// (keys0 keys in all), described on the device by segs0 (in_off, count,
+// final_off set).  A single segment starting at element 0 is laid out here;
+// several segments are laid out by prepare_level_kernel.  Buckets that fit a
+// leaf are sorted straight into their final place in the caller's array.
+template <typename K, typename UserIn, typename UserOut>
+static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint32_t nsegs0, uint64_t keys0,
+                      cudaStream_t st, PhaseTimer& tm, s512_stats& S) {
+    constexpr int KB = sizeof(K);
+    using Shape = PartShape<K>;
+    constexpr int TILE = Shape::THREADS * Shape::IPT;
+    const bool single = nsegs0 == 1;
+
+    // Level buffers T0 / T1 alternate as partition outputs.  A level's output
+    // needs the sum over its segments of region_bound(count) rounded to 16
+    // (prepare_level_kernel lays the segments out that way).
+    K* T[2];
+    const size_t need0 = single ? region_bound(keys0) + 64
+                                : 2 * keys0 + keys0 / 100 + (size_t)nsegs0 * (4096 + 16) + 64;
+    T[0] = (K*)C.get("T0", need0 * KB);
+    T[1] = nullptr;
+    LevelCtl* ctls = (LevelCtl*)C.get("ctl", 2 * sizeof(LevelCtl));
+    LevelCtl* host_ctl = (LevelCtl*)C.host_pinned(sizeof(LevelCtl));
+    const uint32_t next_cap = (uint32_t)(keys0 / leaf_max(KB)) + 2;
+    SegDesc* segbuf[2];
+    segbuf[0] = (SegDesc*)C.get("segs0", (size_t)next_cap * sizeof(SegDesc));
+    segbuf[1] = (SegDesc*)C.get("segs1", (size_t)next_cap * sizeof(SegDesc));
+    if (!T[0] || !ctls || !host_ctl || !segbuf[0] || !segbuf[1]) return S512_ERR_ALLOC;
+
+    // level 0 reads the caller's layout
+    Level<K, UserIn> L0;
+    L0.in = uin;
+    L0.segs = segs0;
+    L0.nsegs = nsegs0;
+    L0.out = T[0];
+    if (single) {
+        L0.tile_seg = nullptr;
+        L0.ntiles_host = (uint32_t)((keys0 + TILE - 1) / TILE);
+        L0.ntiles_dev = nullptr;
+        L0.ntiles_bound = L0.ntiles_host;
+        L0.aligned = true;
+    } else {
+        const uint32_t bound = (uint32_t)(keys0 / TILE) + nsegs0 + 1;
+        uint32_t* tile_seg = (uint32_t*)C.get("tile_seg", (size_t)bound * sizeof(uint32_t));
+        if (!tile_seg) return S512_ERR_ALLOC;
+        S512_CUDA_TRY(cudaMemsetAsync(&ctls[1], 0, sizeof(LevelCtl), st));
+        prepare_level_kernel<<<1, 1024, 0, st>>>(segs0, nsegs0, TILE, &ctls[1]);
+        S512_LAUNCH_CHECK();
+        tile_map_kernel<<<nsegs0, 256, 0, st>>>(segs0, nsegs0, tile_seg);
+        S512_LAUNCH_CHECK();
+        S.kernel_launches += 2;
+        L0.tile_seg = tile_seg;
+        L0.ntiles_host = 0;
+        L0.ntiles_dev = &ctls[1].ntiles_next;
+        L0.ntiles_bound = bound;
+        L0.aligned = false;  // segment starts are wherever the caller's segments start
+    }
+    int rc = run_level<K, UserIn, UserOut>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1], segbuf[1], next_cap, tm,
+                                           S, host_ctl);
+    if (rc) return rc;
+    S.levels = 1;
+
+    uint32_t nsegs = host_ctl->n_next;
+    uint64_t next_keys = host_ctl->next_keys;
+    int level = 1;
+    while (nsegs > 0) {
+        if (level >= 16) {
+            set_error("partition did not converge after %d levels", level);
+            return S512_ERR_INTERNAL;
+        }
+        SegDesc* cur = segbuf[level & 1];
+        SegDesc* nxt = segbuf[(level + 1) & 1];
+        K* in_buf = T[(level - 1) & 1];
+        // grow (never shrink) this level's output buffer; its old contents
+        // were consumed two levels ago
+        const size_t need = 2 * next_keys + next_keys / 100 + (size_t)nsegs * (4096 + 16) + 64;
+        T[level & 1] = (K*)C.get((level & 1) ? "T1" : "T0", need * KB);
+        K* out_buf = T[level & 1];
+        if (!out_buf) return S512_ERR_ALLOC;
+        const uint32_t ntiles_bound = (uint32_t)(next_keys / TILE) + nsegs + 1;
+        uint32_t* tile_seg = (uint32_t*)C.get("tile_seg", (size_t)ntiles_bound * sizeof(uint32_t));
+        if (!tile_seg) return S512_ERR_ALLOC;
+        LevelCtl* lctl = &ctls[level & 1];
+        LevelCtl* tctl = &ctls[(level + 1) & 1];  // receives this level's tile count
+        S512_CUDA_TRY(cudaMemsetAsync(tctl, 0, sizeof(LevelCtl), st));
+        prepare_level_kernel<<<1, 1024, 0, st>>>(cur, nsegs, TILE, tctl);
+        S512_LAUNCH_CHECK();
+        tile_map_kernel<<<nsegs, 256, 0, st>>>(cur, nsegs, tile_seg);
+        S512_LAUNCH_CHECK();
+        S.kernel_launches += 2;
+        Level<K, Raw<K>> Ln;
+        Ln.in = Raw<K>{in_buf, nullptr};
+        Ln.segs = cur;
+        Ln.nsegs = nsegs;
+        Ln.tile_seg = tile_seg;
+        Ln.ntiles_host = 0;
+        Ln.ntiles_dev = &tctl->ntiles_next;
+        Ln.ntiles_bound = ntiles_bound;
+        Ln.out = out_buf;
+        Ln.aligned = true;
+        // the tile count lives in tctl, so the level's own control block is the other one
+        rc = run_level<K, Raw<K>, UserOut>(C, Ln, level, uout, keys0, st, lctl, tctl, nxt, next_cap, tm, S,
+                                           host_ctl);
+        if (rc) return rc;
+        if (level < S512_MAX_LEVELS) S.partition_keys[level] += next_keys;
+        nsegs = host_ctl->n_next;
+        next_keys = host_ctl->next_keys;
+        ++level;
+        S.levels = level;
+    }
+    return S512_OK;
+}
+
+// The whole pipeline for one array of n > leaf_max keys.
+template <typename K, typename UserIn, typename UserOut>
+static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st) {
+    constexpr int TILE = PartShape<K>::THREADS * PartShape<K>::IPT;
+    s512_stats& S = thread_stats();
+    PhaseTimer tm(st, config().collect_stats != 0);
+    const int tstart = tm.mark();
+    SegDesc* seg0 = (SegDesc*)C.get("seg_whole", sizeof(SegDesc));
+    if (!seg0) return S512_ERR_ALLOC;
+    SegDesc s0;
+    s0.in_off = 0;
+    s0.count = n;
+    s0.final_off = 0;
+    s0.out_base = 0;
+    s0.tile_start = 0;
+    s0.ntiles = (uint32_t)((n + TILE - 1) / TILE);
+    S512_CUDA_TRY(cudaMemcpyAsync(seg0, &s0, sizeof(SegDesc), cudaMemcpyHostToDevice, st));
+    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S);
+    if (rc) return rc;
+    const int tend = tm.mark();
+    if (tm.on()) S.total_ms = tm.ms(tstart, tend);
+    return S512_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Entry: sort `n` keys read through uin and written through uout (same
+// positions; device memory).
+template <typename K, typename UserIn, typename UserOut>
+static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st) {
+    s512_stats& S = thread_stats();
+    memset(&S, 0, sizeof(S));
+    S.key_bytes = sizeof(K);
+    if (n <= 1) {
+        if (n == 1) {
+            // still route through the codec so in != out works
+            int rc = sort_one_leaf<UserIn, UserOut>(C, uin, uout, 1, st);
+            S.kernel_launches = 1;
+            return rc;
+        }
+        return S512_OK;
+    }
+    if (n <= leaf_max(sizeof(K))) {
+        PhaseTimer tm(st, config().collect_stats != 0);
+        const int a = tm.mark();
+        int rc = sort_one_leaf<UserIn, UserOut>(C, uin, uout, (uint32_t)n, st);
+        const int b = tm.mark();
+        S.kernel_launches = 1;
+        if (tm.on()) S.total_ms = tm.ms(a, b);
+        return rc;
+    }
+    return sort_pipeline<K, UserIn, UserOut>(C, uin, uout, n, st);
+}
+
+// ---------------------------------------------------------------------------
+// Host-pointer staging: copy to a device buffer, run `fn`, copy back.
+struct HostStage {
+    void* dev[2] = {nullptr, nullptr};
+};
+
+static int finish_call(CallGuard& g, cudaStream_t st, int flags, bool host) {
+    g.finish();
+    if (host || !(flags & S512_ASYNC)) S512_CUDA_TRY(cudaStreamSynchronize(st));
+    return S512_OK;
+}
+
+}  // namespace s512
+

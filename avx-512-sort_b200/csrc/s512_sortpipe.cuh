@@ -753,7 +753,7 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
 }
 
 // Give the next level's segments their tiles and output regions (one block).
-__global__ void __launch_bounds__(1024) prepare_level_kernel(SegDesc* segs, uint32_t nsegs, uint32_t tile,
+static __global__ void __launch_bounds__(1024) prepare_level_kernel(SegDesc* segs, uint32_t nsegs, uint32_t tile,
                                                              LevelCtl* ctl_next) {
     __shared__ uint64_t wt1[32], wt2[32];
     __shared__ uint64_t tot1, tot2;
@@ -791,7 +791,7 @@ __global__ void __launch_bounds__(1024) prepare_level_kernel(SegDesc* segs, uint
 }
 
 // tile -> segment map (one block per segment)
-__global__ void tile_map_kernel(const SegDesc* segs, uint32_t nsegs, uint32_t* tile_seg) {
+static __global__ void tile_map_kernel(const SegDesc* segs, uint32_t nsegs, uint32_t* tile_seg) {
     const uint32_t s = blockIdx.x;
     if (s >= nsegs) return;
     const SegDesc sd = segs[s];

@@ -44,7 +44,11 @@ EXPORTS = (
     "s512_popcount",
     "s512_partition_i32_noalloc",
     "s512_merge_i32", "s512_merge_f64", "s512_sort_omp_merge_i32", "s512_sort_omp_merge_f64",
+    "s512_segsort_i32", "s512_segsort_f64", "s512_segsort_kv_i32", "s512_segsort_tune",
+    "s512_segsort_plan_create", "s512_segsort_plan_launch", "s512_segsort_plan_destroy",
 )
+
+DTYPE_I32, DTYPE_F64, DTYPE_KV_I32 = 0, 1, 2
 
 
 class Config(ctypes.Structure):
@@ -134,6 +138,12 @@ def lib() -> ctypes.CDLL:
     for suf in ("i32", "f64"):
         getattr(L, f"s512_merge_{suf}").argtypes = [vp, sz, sz, ci, vp]
         getattr(L, f"s512_sort_omp_merge_{suf}").argtypes = [vp, sz, ci, ci, vp]
+        getattr(L, f"s512_segsort_{suf}").argtypes = [vp, vp, sz, ci, vp]
+    L.s512_segsort_kv_i32.argtypes = [vp, vp, vp, sz, ci, vp]
+    L.s512_segsort_tune.argtypes = [ci, vp, sz, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ci), vp]
+    L.s512_segsort_plan_create.argtypes = [ctypes.POINTER(vp), ci, vp, vp, vp, sz, vp]
+    L.s512_segsort_plan_launch.argtypes = [vp, vp]
+    L.s512_segsort_plan_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -220,6 +230,66 @@ def sort_omp_merge(a, nparts: int = 8, flags: int = 0, stream=None) -> None:
     p, n, dt, dev = _ptr(a)
     fn = f"s512_sort_omp_merge_{_suffix(dt)}"
     _check(fn, getattr(lib(), fn)(p, n, nparts, _flags(dev, flags), _stream(stream)))
+
+
+# -- batched segmented sort ----------------------------------------------------
+def _offsets_ptr(offsets):
+    if isinstance(offsets, np.ndarray):
+        if offsets.dtype != np.uint64 or not offsets.flags.c_contiguous:
+            raise ValueError("offsets must be a contiguous uint64 array")
+        return offsets.ctypes.data, offsets.size - 1
+    return offsets.data_ptr(), offsets.numel() - 1  # torch int64 tensor on the device
+
+
+def segsort(a, offsets, flags: int = 0, stream=None) -> None:
+    """Sort every segment a[offsets[s]:offsets[s+1]] in place."""
+    p, n, dt, dev = _ptr(a)
+    po, nseg = _offsets_ptr(offsets)
+    fn = f"s512_segsort_{_suffix(dt)}"
+    _check(fn, getattr(lib(), fn)(p, po, nseg, _flags(dev, flags), _stream(stream)))
+
+
+def segsort_kv(keys, values, offsets, flags: int = 0, stream=None) -> None:
+    pk, n, _, dev = _ptr(keys)
+    pv, _, _, _ = _ptr(values)
+    po, nseg = _offsets_ptr(offsets)
+    _check("s512_segsort_kv_i32", lib().s512_segsort_kv_i32(pk, pv, po, nseg, _flags(dev, flags), _stream(stream)))
+
+
+def segsort_tune(dtype: int, d_offsets, stream=None):
+    """Time the persistent launch's shapes on this layout; returns (best_ms, shape)."""
+    po, nseg = _offsets_ptr(d_offsets)
+    ms = ctypes.c_double(0)
+    shape = ctypes.c_int(-1)
+    _check("s512_segsort_tune", lib().s512_segsort_tune(dtype, po, nseg, ctypes.byref(ms), ctypes.byref(shape),
+                                                        _stream(stream)))
+    return ms.value, shape.value
+
+
+class SegsortPlan:
+    """A segmented sort captured in a CUDA graph (device buffers only)."""
+
+    def __init__(self, dtype: int, keys, d_offsets, values=None, stream=None):
+        self.h = ctypes.c_void_p(0)
+        po, nseg = _offsets_ptr(d_offsets)
+        pk = keys.data_ptr()
+        pv = values.data_ptr() if values is not None else None
+        _check("s512_segsort_plan_create", lib().s512_segsort_plan_create(ctypes.byref(self.h), dtype, pk, pv, po,
+                                                                          nseg, _stream(stream)))
+
+    def launch(self, stream=None) -> None:
+        _check("s512_segsort_plan_launch", lib().s512_segsort_plan_launch(self.h, _stream(stream)))
+
+    def close(self) -> None:
+        if self.h:
+            lib().s512_segsort_plan_destroy(self.h)
+            self.h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
 
 
 # -- Sort512kv ----------------------------------------------------------------
