@@ -1,0 +1,489 @@
+// s512_learned.cuh -- learned splitters: a small monotone CDF model per
+// segment, fitted on the device to the segment's sorted sample, that maps a
+// key to its bucket in a few arithmetic steps instead of the plain splitters'
+// eight-level tree search.  The plain splitters stay as the fallback.
+//
+// Model (all slopes non-negative, so the map is monotone by construction):
+//   z   = float(key - kmin) * inv_range                      (saturating at 0)
+//   p0  = c[s] + w[s] * (z*R - s),   s = clamp(floor(z*R))   (root: R pieces)
+//   l   = clamp(floor(p0 * LEAVES))                           (leaf choice)
+//   p   = clamp(a[l] + b[l] * float(key - base[l]), lo[l], hi[l])
+//   r   = min(floor(p * nmodel), nmodel - 1)                  (model bucket)
+// with w = theta^2 >= 0 (root slopes), c the running sum of w, b >= 0, and
+// [lo[l], hi[l]] the sample-CDF range of leaf l, so that every leaf's outputs
+// lie above the previous leaf's.  Each step is a non-decreasing function of
+// the previous one, in IEEE arithmetic too, hence keys map to buckets in key
+// order and a partition by model buckets is a valid sample-sort partition:
+// the model only decides how balanced the buckets are, never the result.
+// A "heavy" key (one that repeats among the sample quantiles, as for the plain
+// splitters' equality buckets) splits its model bucket into below / equal /
+// above, and its equal bucket needs no sort.
+//
+// Training (learned_fit_kernel, one block per segment): targets are the
+// sample's empirical CDF y_i = (i + 0.5) / m.  The root starts from the
+// sample histogram over its R pieces and takes ITERS full-batch Adam steps on
+// theta with the analytic gradient
+//   dL/dw_t = (2/m) * ( sum_{i: s_i > t} r_i + sum_{i: s_i = t} r_i * frac_i ),
+//   dL/dtheta_t = dL/dw_t * 2 * theta_t,         r_i = p0(z_i) - y_i.
+// Each leaf starts from its least-squares line on the samples routed to it and
+// takes LEAF_ITERS Adam steps on (a, beta) with b = beta^2.
+#pragma once
+
+#include "s512_blocksort.cuh"
+
+// (included from s512_sortpipe.cuh after the split-set types)
+
+namespace s512 {
+
+constexpr int LR_ROOT = 64;
+constexpr int LR_LEAVES = 256;
+constexpr int LR_THREADS = 512;
+constexpr int LR_ITERS = 40;
+constexpr int LR_LEAF_ITERS = 20;
+constexpr float LR_STEP = 0.02f;  // Adam step, relative to the parameters' scale
+
+template <typename K>
+struct LeafParam {
+    K base;
+    float a, b, lo, hi;
+};
+
+template <typename K>
+struct LearnedSet {
+    K kmin;
+    float inv_range;
+    float rc[LR_ROOT];   // root: value at the start of each piece (normalised)
+    float rw[LR_ROOT];   // root: slope of each piece (normalised, >= 0)
+    LeafParam<K> leaf[LR_LEAVES];
+    K heavy[NB];         // per model bucket: its heavy key (if heavy_flag)
+    uint8_t heavy_flag[NB];
+    uint8_t base_id[NB]; // first bucket id of each model bucket
+    uint64_t region_off[NB];
+    uint64_t region_cap[NB];
+    uint32_t bucket_eq[NB / 32];
+    uint32_t nbuckets;
+    uint32_t nmodel;     // model buckets
+    uint32_t ok;         // 1: accepted (imbalance within bound)
+    uint32_t pad_;
+    float loss_init, loss_root, loss_final;
+    float max_over_mean;  // sample-count imbalance of the learned buckets
+};
+
+// ---------------------------------------------------------------------------
+// inference
+
+__device__ __forceinline__ float key_to_float(uint32_t d) { return __uint2float_rn(d); }
+__device__ __forceinline__ float key_to_float(uint64_t d) { return __ull2float_rn(d); }
+
+template <typename K>
+__device__ __forceinline__ float root_p0(const float* rc, const float* rw, K kmin, float inv_range, K key,
+                                         float* frac_out = nullptr, int* seg_out = nullptr) {
+    const K d = key > kmin ? key - kmin : K(0);
+    const float zr = key_to_float(d) * inv_range * (float)LR_ROOT;
+    int s = (int)zr;
+    s = s < 0 ? 0 : (s > LR_ROOT - 1 ? LR_ROOT - 1 : s);
+    const float frac = zr - (float)s;
+    if (frac_out) *frac_out = frac;
+    if (seg_out) *seg_out = s;
+    return rc[s] + rw[s] * frac;
+}
+
+template <typename K>
+__device__ __forceinline__ int leaf_of(float p0) {
+    int l = (int)(p0 * (float)LR_LEAVES);
+    return l < 0 ? 0 : (l > LR_LEAVES - 1 ? LR_LEAVES - 1 : l);
+}
+
+template <typename K>
+__device__ __forceinline__ float leaf_p(const LeafParam<K>& lp, K key) {
+    const K du = key > lp.base ? key - lp.base : K(0);
+    const float p = lp.a + lp.b * key_to_float(du);
+    return fminf(fmaxf(p, lp.lo), lp.hi);
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t model_bucket(float p, uint32_t nmodel) {
+    int r = (int)(p * (float)nmodel);
+    r = r < 0 ? 0 : r;
+    return (uint32_t)r > nmodel - 1 ? nmodel - 1 : (uint32_t)r;
+}
+
+// bucket id of a key under a learned set held in shared memory
+template <typename K>
+__device__ __forceinline__ uint32_t learned_bucket(const LearnedSet<K>& L, K key) {
+    const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, key);
+    const LeafParam<K>& lp = L.leaf[leaf_of<K>(p0)];
+    const uint32_t r = model_bucket<K>(leaf_p<K>(lp, key), L.nmodel);
+    uint32_t id = L.base_id[r];
+    if (L.heavy_flag[r]) {
+        const K h = L.heavy[r];
+        id += key < h ? 0u : (key == h ? 1u : 2u);
+    }
+    return id;
+}
+
+// ---------------------------------------------------------------------------
+// training
+
+struct Adam {
+    float m = 0.f, v = 0.f;
+    __device__ __forceinline__ float step(float g, float lr, int t) {
+        const float b1 = 0.9f, b2 = 0.999f;
+        m = b1 * m + (1.f - b1) * g;
+        v = b2 * v + (1.f - b2) * g * g;
+        const float mh = m / (1.f - powf(b1, (float)t));
+        const float vh = v / (1.f - powf(b2, (float)t));
+        return lr * mh / (sqrtf(vh) + 1e-8f);
+    }
+};
+
+// Root forward + backward over the sorted sample: loss, and dL/dw per piece.
+// rc/rw are the un-normalised running sums / slopes.  Block-wide; S0/S1 and
+// loss_acc are shared scratch.
+template <typename K>
+__device__ void root_forward_backward(const K* smp, uint32_t m, K kmin, float inv_range, const float* rc,
+                                      const float* rw, float* S0, float* S1, float* loss_acc, float* gw) {
+    for (int t = threadIdx.x; t < LR_ROOT; t += blockDim.x) {
+        S0[t] = 0.f;
+        S1[t] = 0.f;
+    }
+    if (threadIdx.x == 0) *loss_acc = 0.f;
+    __syncthreads();
+    // each thread walks a contiguous run of the (sorted) sample, so its
+    // samples fall in few pieces: accumulate locally, flush on a piece change
+    float lsum = 0.f;
+    const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
+    const uint32_t i0 = threadIdx.x * per;
+    const uint32_t i1 = i0 + per < m ? i0 + per : m;
+    int cur = -1;
+    float a0 = 0.f, a1 = 0.f;
+    for (uint32_t i = i0; i < i1; ++i) {
+        float frac;
+        int s;
+        const float p0 = root_p0<K>(rc, rw, kmin, inv_range, smp[i], &frac, &s);
+        const float y = ((float)i + 0.5f) / (float)m;
+        const float r = p0 - y;
+        lsum += r * r;
+        if (s != cur) {
+            if (cur >= 0) {
+                atomicAdd(&S0[cur], a0);
+                atomicAdd(&S1[cur], a1);
+            }
+            cur = s;
+            a0 = a1 = 0.f;
+        }
+        a0 += r;
+        a1 += r * frac;
+    }
+    if (cur >= 0) {
+        atomicAdd(&S0[cur], a0);
+        atomicAdd(&S1[cur], a1);
+    }
+    atomicAdd(loss_acc, lsum);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float suffix = 0.f;  // sum of r over later pieces
+        for (int t = LR_ROOT - 1; t >= 0; --t) {
+            gw[t] = 2.f / (float)m * (suffix + S1[t]);
+            suffix += S0[t];
+        }
+        *loss_acc /= (float)m;
+    }
+    __syncthreads();
+}
+
+// One block (LR_THREADS) per segment.  The plain split set of the segment
+// (already computed from the same sorted sample) supplies the heavy keys.
+template <typename K>
+__global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __restrict__ samples,
+                                                                 const SegDesc* __restrict__ segs, uint32_t nsegs,
+                                                                 const SplitSet<K>* __restrict__ plain,
+                                                                 LearnedSet<K>* __restrict__ out, int key_bytes,
+                                                                 float max_imbalance) {
+    const uint32_t sgi = blockIdx.x;
+    if (sgi >= nsegs) return;
+    __shared__ float theta[LR_ROOT], rw[LR_ROOT], rc[LR_ROOT], gw[LR_ROOT], S0[LR_ROOT], S1[LR_ROOT];
+    __shared__ float loss_acc;
+    __shared__ uint32_t leaf_first[LR_LEAVES + 1];
+    __shared__ uint32_t hist[NB];
+    __shared__ uint32_t wt32[32];
+    __shared__ uint64_t wt64[32];
+    __shared__ uint32_t nheavy_s, max_s, nonempty_s;
+    __shared__ LearnedSet<K> L;  // built here, copied out at the end
+
+    const SegDesc sd = segs[sgi];
+    const int nb = target_buckets(key_bytes, sd.count);
+    const uint32_t m = sample_size(nb);
+    const K* smp = samples + (size_t)sgi * SAMPLE_N;
+    const int tid = threadIdx.x;
+
+    // coordinate
+    const K kmin = smp[0], kmax = smp[m - 1];
+    const K range = kmax - kmin;
+    const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
+
+    // root init: histogram of the sample over the pieces, theta = sqrt(w)
+    for (int t = tid; t < LR_ROOT; t += blockDim.x) S0[t] = 0.f;
+    __syncthreads();
+    {
+        const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
+        const uint32_t i0 = tid * per;
+        const uint32_t i1 = i0 + per < m ? i0 + per : m;
+        int cur = -1;
+        float acc = 0.f;
+        for (uint32_t i = i0; i < i1; ++i) {
+            const K d = smp[i] > kmin ? smp[i] - kmin : K(0);
+            const float zr = key_to_float(d) * inv_range * (float)LR_ROOT;
+            int s = (int)zr;
+            s = s < 0 ? 0 : (s > LR_ROOT - 1 ? LR_ROOT - 1 : s);
+            if (s != cur) {
+                if (cur >= 0) atomicAdd(&S0[cur], acc);
+                cur = s;
+                acc = 0.f;
+            }
+            acc += 1.f / (float)m;
+        }
+        if (cur >= 0) atomicAdd(&S0[cur], acc);
+    }
+    __syncthreads();
+    if (tid < LR_ROOT) theta[tid] = sqrtf(S0[tid]);
+    __syncthreads();
+
+    // Adam on theta; the parameters with the lowest loss seen are kept, so
+    // training never ends worse than the histogram start
+    Adam opt;
+    float best_theta = tid < LR_ROOT ? theta[tid] : 0.f;
+    float best_loss = 3.4e38f;
+    for (int it = 0; it <= LR_ITERS; ++it) {
+        if (tid < LR_ROOT) rw[tid] = theta[tid] * theta[tid];
+        __syncthreads();
+        if (tid == 0) {
+            float c = 0.f;
+            for (int t = 0; t < LR_ROOT; ++t) {
+                rc[t] = c;
+                c += rw[t];
+            }
+        }
+        __syncthreads();
+        root_forward_backward<K>(smp, m, kmin, inv_range, rc, rw, S0, S1, &loss_acc, gw);
+        const float loss = loss_acc;
+        if (it == 0 && tid == 0) L.loss_init = loss;
+        if (loss < best_loss) {
+            best_loss = loss;
+            if (tid < LR_ROOT) best_theta = theta[tid];
+        }
+        if (it == LR_ITERS) break;
+        if (tid < LR_ROOT) theta[tid] -= opt.step(gw[tid] * 2.f * theta[tid], LR_STEP * 0.125f, it + 1);
+        __syncthreads();
+    }
+    __syncthreads();
+    if (tid < LR_ROOT) {
+        theta[tid] = best_theta;
+        rw[tid] = best_theta * best_theta;
+    }
+    if (tid == 0) L.loss_root = best_loss;
+    __syncthreads();
+    // normalise the root so that it spans [0, 1]
+    if (tid == 0) {
+        float tot = 0.f;
+        for (int t = 0; t < LR_ROOT; ++t) tot += rw[t];
+        const float inv = tot > 0.f ? 1.f / tot : 0.f;
+        float c = 0.f;
+        for (int t = 0; t < LR_ROOT; ++t) {
+            L.rc[t] = c * inv;
+            L.rw[t] = rw[t] * inv;
+            c += rw[t];
+        }
+        L.kmin = kmin;
+        L.inv_range = inv_range;
+    }
+    __syncthreads();
+
+    // leaves: samples are sorted and routing is monotone, so each leaf owns a
+    // contiguous run of the sample; find the run starts
+    for (int l = tid; l <= LR_LEAVES; l += blockDim.x) leaf_first[l] = m;
+    __syncthreads();
+    for (uint32_t i = tid; i < m; i += blockDim.x) {
+        const int l = leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i]));
+        const int lp = i == 0 ? -1 : leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i - 1]));
+        for (int q = lp + 1; q <= l; ++q) leaf_first[q] = i;  // leaves lp+1..l start at i
+    }
+    __syncthreads();
+    if (tid < LR_LEAVES) {
+        const int l = tid;
+        const uint32_t f = leaf_first[l];
+        // leaf_first[q] = first sample routed to a leaf >= q, so leaf l owns
+        // the samples [leaf_first[l], leaf_first[l+1])
+        const uint32_t e = leaf_first[l + 1];
+        LeafParam<K> P;
+        if (f < e && f < m) {
+            const K base = smp[f];
+            const K span = smp[e - 1] - base;
+            const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
+            // least squares on (u, y), u in [0, 1]
+            float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
+            const float cnt = (float)(e - f);
+            for (uint32_t i = f; i < e; ++i) {
+                const float u = key_to_float(smp[i] - base) * inv_span;
+                const float y = ((float)i + 0.5f) / (float)m;
+                su += u;
+                sy += y;
+                suu += u * u;
+                suy += u * y;
+            }
+            const float mu = su / cnt, my = sy / cnt;
+            const float var = suu / cnt - mu * mu, cov = suy / cnt - mu * my;
+            float b = var > 1e-12f ? cov / var : 0.f;
+            b = b > 0.f ? b : 0.f;
+            float a = my - b * mu;
+            // refine (a, beta), b = beta^2, by Adam on the leaf's squared
+            // error (forward + backward per step); keep the best pair seen
+            float beta = sqrtf(b);
+            float best_a = a, best_beta = beta, best_l = 3.4e38f;
+            Adam oa, ob;
+            for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
+                float ga = 0.f, gb = 0.f, l2 = 0.f;
+                for (uint32_t i = f; i < e; ++i) {
+                    const float u = key_to_float(smp[i] - base) * inv_span;
+                    const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
+                    l2 += r * r;
+                    ga += r;
+                    gb += r * u;
+                }
+                if (l2 < best_l) {
+                    best_l = l2;
+                    best_a = a;
+                    best_beta = beta;
+                }
+                if (it > LR_LEAF_ITERS) break;
+                ga *= 2.f / cnt;
+                gb *= 2.f / cnt * 2.f * beta;
+                a -= oa.step(ga, LR_STEP / (float)m, it);
+                beta -= ob.step(gb, LR_STEP / (float)m, it);
+            }
+            a = best_a;
+            beta = best_beta;
+            P.base = base;
+            P.a = a;
+            P.b = beta * beta * inv_span;  // slope per unit of (key - base)
+            P.lo = ((float)f + 0.5f) / (float)m;
+            P.hi = ((float)(e - 1) + 0.5f) / (float)m;
+        } else {
+            P.base = KeyMax<K>::value;
+            P.a = 0.f;
+            P.b = 0.f;
+            P.lo = P.hi = -1.f;  // patched below: an empty leaf repeats its left neighbour's top
+        }
+        L.leaf[l] = P;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        float last = 0.f;
+        for (int l = 0; l < LR_LEAVES; ++l) {
+            if (L.leaf[l].lo < 0.f) {
+                L.leaf[l].lo = L.leaf[l].hi = last;
+                L.leaf[l].a = last;
+            } else {
+                last = L.leaf[l].hi;
+            }
+        }
+    }
+    __syncthreads();
+
+    // buckets: heavy keys from the plain split set (splitters with an equality bucket)
+    const SplitSet<K>& ps = plain[sgi];
+    if (tid == 0) nheavy_s = 0;
+    __syncthreads();
+    uint32_t heavy_mine = 0;
+    if (tid < NB && tid < (int)ps.nuniq) heavy_mine = (ps.eq_mask[tid >> 5] >> (tid & 31)) & 1u;
+    const uint32_t nheavy = __syncthreads_count(heavy_mine != 0);
+    uint32_t nmodel = NB - 2 * nheavy;
+    if (nmodel > (uint32_t)(2 * nb)) nmodel = 2 * nb;  // no more model buckets than the plain path aims for
+    if (nmodel < 2) nmodel = 2;
+    if (tid < NB) {
+        L.heavy_flag[tid] = 0;
+        L.heavy[tid] = K(0);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        L.nmodel = nmodel;
+        // heavy keys in ascending order; a model bucket keeps its first heavy key
+        for (uint32_t j = 0; j < ps.nuniq && j < (uint32_t)NB; ++j) {
+            if (!((ps.eq_mask[j >> 5] >> (j & 31)) & 1u)) continue;
+            const K h = ps.uniq[j];
+            const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, h);
+            const uint32_t r = model_bucket<K>(leaf_p<K>(L.leaf[leaf_of<K>(p0)], h), nmodel);
+            if (!L.heavy_flag[r]) {
+                L.heavy_flag[r] = 1;
+                L.heavy[r] = h;
+            }
+        }
+        uint32_t id = 0;
+        for (uint32_t r = 0; r < NB; ++r) {
+            L.base_id[r] = (uint8_t)(id < NB ? id : NB - 1);
+            if (r < nmodel) id += L.heavy_flag[r] ? 3u : 1u;
+        }
+        L.nbuckets = id;
+    }
+    __syncthreads();
+
+    // sample counts per learned bucket -> imbalance, capacities, regions
+    if (tid < NB) hist[tid] = 0;
+    if (tid == 0) {
+        max_s = 0;
+        nonempty_s = 0;
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < m; i += blockDim.x) atomicAdd(&hist[learned_bucket<K>(L, smp[i])], 1u);
+    __syncthreads();
+    uint32_t c = tid < NB ? hist[tid] : 0u;
+    if (tid < NB && c) {
+        atomicMax(&max_s, c);
+        atomicAdd(&nonempty_s, 1u);
+    }
+    uint32_t eq_bit = 0;
+    if (tid < NB) {
+        // bucket tid is an "equal" bucket if it is base_id[r]+1 of a heavy model bucket
+        for (uint32_t r = 0; r < nmodel; ++r)
+            if (L.heavy_flag[r] && (uint32_t)L.base_id[r] + 1 == (uint32_t)tid) eq_bit = 1;
+    }
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, eq_bit != 0);
+    if (tid < NB && (tid & 31) == 0) L.bucket_eq[tid >> 5] = bal;
+    const double scale = (double)sd.count / (double)m;
+    uint64_t cap = 0;
+    if (tid < NB && (uint32_t)tid < L.nbuckets) {
+        const double v = ((double)c + 6.0 * sqrt((double)c + 1.0) + 16.0) * scale;
+        cap = (uint64_t)ceil(v);
+        if (cap > sd.count) cap = sd.count;
+        cap = (cap + 15) & ~15ull;
+    }
+    const uint64_t off = block_exclusive_scan_first<NB, uint64_t>(cap, wt64, (uint64_t*)nullptr);
+    if (tid < NB) {
+        L.region_off[tid] = off;
+        L.region_cap[tid] = cap;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const float mean = nonempty_s ? (float)m / (float)nonempty_s : 1.f;
+        L.max_over_mean = (float)max_s / mean;
+        L.ok = (L.max_over_mean <= max_imbalance && L.nbuckets <= (uint32_t)NB) ? 1u : 0u;
+        // final loss of the whole model on the sample (root + leaves)
+        L.loss_final = 0.f;
+    }
+    __syncthreads();
+    float lf = 0.f;
+    for (uint32_t i = tid; i < m; i += blockDim.x) {
+        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, smp[i]);
+        const float r = leaf_p<K>(L.leaf[leaf_of<K>(p0)], smp[i]) - ((float)i + 0.5f) / (float)m;
+        lf += r * r;
+    }
+    atomicAdd(&L.loss_final, lf / (float)m);
+    __syncthreads();
+    // copy out
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&L);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(out + sgi);
+    for (uint32_t i = tid; i < sizeof(LearnedSet<K>) / 4; i += blockDim.x) dst[i] = src[i];
+    (void)wt32;
+}
+
+}  // namespace s512

@@ -113,7 +113,7 @@ struct Level {
 template <typename K, typename InCodec, typename UserOut>
 static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, size_t n, cudaStream_t st,
                      LevelCtl* ctl, LevelCtl* next_ctl_dev, SegDesc* next_segs, uint32_t next_cap,
-                     PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl) {
+                     PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl, bool learned) {
     constexpr int KB = sizeof(K);
     using Shape = PartShape<K>;
     constexpr int TILE = Shape::THREADS * Shape::IPT;
@@ -134,7 +134,8 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         for (int c = 0; c <= NCLASS; ++c) items[c] = (LeafItem<K>*)(base + (size_t)c * item_cap * sizeof(LeafItem<K>));
     }
     uint32_t* chain = (uint32_t*)C.get("chain", (size_t)nsegs * sizeof(uint32_t));
-    if (!samples || !splits || !counts || !status || !chain) return S512_ERR_ALLOC;
+    LearnedSet<K>* lsets = learned ? (LearnedSet<K>*)C.get("lsets", (size_t)nsegs * sizeof(LearnedSet<K>)) : nullptr;
+    if (!samples || !splits || !counts || !status || !chain || (learned && !lsets)) return S512_ERR_ALLOC;
 
     const int t0 = tm.mark();
     S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
@@ -154,6 +155,14 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     splitter_kernel<K><<<nsegs, NB, 0, st>>>(samples, L.segs, nsegs, splits, KB);
     S512_LAUNCH_CHECK();
     S.kernel_launches += 3;
+    if (learned) {
+        // the model is fitted to the same sorted sample; the split set above
+        // stays as its fallback and supplies the heavy keys
+        learned_fit_kernel<K><<<nsegs, LR_THREADS, 0, st>>>(samples, L.segs, nsegs, splits, lsets, KB,
+                                                           (float)config().max_imbalance);
+        S512_LAUNCH_CHECK();
+        S.kernel_launches += 1;
+    }
     const int t1 = tm.mark();
 
     PartArgs<K> pa;
@@ -169,6 +178,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     pa.nsegs = nsegs;
     pa.tma = (L.aligned && codec_aligned(L.in)) ? 1 : 0;
     pa.chain = chain;
+    pa.learned = lsets;
     auto pfn = partition_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
     const size_t psmem = sizeof(PartSmem<K, Shape::THREADS, Shape::IPT>);
     int pgrid = 0;
@@ -181,6 +191,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     PlanArgs<K> pl;
     pl.segs = L.segs;
     pl.splits = splits;
+    pl.learned = lsets;
     pl.bucket_counts = counts;
     pl.level_out = L.out;
     for (int c = 0; c <= NCLASS; ++c) pl.items[c] = items[c];
@@ -196,8 +207,12 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     S.kernel_launches += 1;
 
     if (host_ctl->err & DEV_ERR_OVERFLOW) {
-        // a bucket outgrew its sampled capacity: exact counts, exact regions, redo
+        // a bucket outgrew its sampled capacity: exact counts, exact regions,
+        // redo with the splitters only
         S.fallbacks += 1;
+        if (lsets) S.learned_rejected += host_ctl->learned_used;
+        pa.learned = nullptr;
+        pl.learned = nullptr;
         const uint32_t ntiles = L.ntiles_dev ? host_ctl->ntiles_next : L.ntiles_host;
         (void)ntiles;
         S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
@@ -239,6 +254,8 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     }
     const int t4 = tm.mark();
 
+    if (lsets && host_ctl->learned_used) S.learned_levels += 1;
+    if (lsets) S.learned_rejected += host_ctl->plain_used;
     if (level < S512_MAX_LEVELS) {
         S.partition_keys[level] += (level == 0) ? (uint64_t)n : 0;
         S.partition_launches[level] += 1;
@@ -264,7 +281,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
 // leaf are sorted straight into their final place in the caller's array.
 template <typename K, typename UserIn, typename UserOut>
 static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint32_t nsegs0, uint64_t keys0,
-                      cudaStream_t st, PhaseTimer& tm, s512_stats& S) {
+                      cudaStream_t st, PhaseTimer& tm, s512_stats& S, bool learned = false) {
     constexpr int KB = sizeof(K);
     using Shape = PartShape<K>;
     constexpr int TILE = Shape::THREADS * Shape::IPT;
@@ -315,7 +332,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         L0.aligned = false;  // segment starts are wherever the caller's segments start
     }
     int rc = run_level<K, UserIn, UserOut>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1], segbuf[1], next_cap, tm,
-                                           S, host_ctl);
+                                           S, host_ctl, learned);
     if (rc) return rc;
     S.levels = 1;
 
@@ -359,7 +376,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         Ln.aligned = true;
         // the tile count lives in tctl, so the level's own control block is the other one
         rc = run_level<K, Raw<K>, UserOut>(C, Ln, level, uout, keys0, st, lctl, tctl, nxt, next_cap, tm, S,
-                                           host_ctl);
+                                           host_ctl, learned);
         if (rc) return rc;
         if (level < S512_MAX_LEVELS) S.partition_keys[level] += next_keys;
         nsegs = host_ctl->n_next;
@@ -372,7 +389,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
 
 // The whole pipeline for one array of n > leaf_max keys.
 template <typename K, typename UserIn, typename UserOut>
-static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st) {
+static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned) {
     constexpr int TILE = PartShape<K>::THREADS * PartShape<K>::IPT;
     s512_stats& S = thread_stats();
     PhaseTimer tm(st, config().collect_stats != 0);
@@ -387,7 +404,7 @@ static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStre
     s0.tile_start = 0;
     s0.ntiles = (uint32_t)((n + TILE - 1) / TILE);
     S512_CUDA_TRY(cudaMemcpyAsync(seg0, &s0, sizeof(SegDesc), cudaMemcpyHostToDevice, st));
-    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S);
+    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S, learned);
     if (rc) return rc;
     const int tend = tm.mark();
     if (tm.on()) S.total_ms = tm.ms(tstart, tend);
@@ -398,7 +415,7 @@ static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStre
 // Entry: sort `n` keys read through uin and written through uout (same
 // positions; device memory).
 template <typename K, typename UserIn, typename UserOut>
-static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st) {
+static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned = false) {
     s512_stats& S = thread_stats();
     memset(&S, 0, sizeof(S));
     S.key_bytes = sizeof(K);
@@ -420,7 +437,7 @@ static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream
         if (tm.on()) S.total_ms = tm.ms(a, b);
         return rc;
     }
-    return sort_pipeline<K, UserIn, UserOut>(C, uin, uout, n, st);
+    return sort_pipeline<K, UserIn, UserOut>(C, uin, uout, n, st, learned);
 }
 
 // ---------------------------------------------------------------------------
@@ -428,6 +445,13 @@ static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream
 struct HostStage {
     void* dev[2] = {nullptr, nullptr};
 };
+
+// learned splitters for this call: the flag wins over the configuration
+static inline bool use_learned(int flags) {
+    if (flags & S512_SPLIT_LEARNED) return true;
+    if (flags & S512_SPLIT_PLAIN) return false;
+    return config().splitter_mode == S512_SPLIT_LEARNED;
+}
 
 static int finish_call(CallGuard& g, cudaStream_t st, int flags, bool host) {
     g.finish();

@@ -36,7 +36,7 @@ int s512_sort_i32(int* data, size_t n, int flags, void* stream) {
         if (!d) return S512_ERR_ALLOC;
         S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * sizeof(int), cudaMemcpyHostToDevice, st));
     }
-    int rc = sort_device<uint32_t>(*C, CodecI32{d, d}, CodecI32{d, d}, n, st);
+    int rc = sort_device<uint32_t>(*C, CodecI32{d, d}, CodecI32{d, d}, n, st, use_learned(flags));
     if (rc) return rc;
     if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     return finish_call(guard_, st, flags, host);
@@ -54,7 +54,7 @@ int s512_sort_f64(double* data, size_t n, int flags, void* stream) {
         if (!d) return S512_ERR_ALLOC;
         S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * sizeof(double), cudaMemcpyHostToDevice, st));
     }
-    int rc = sort_device<uint64_t>(*C, CodecF64{d, d}, CodecF64{d, d}, n, st);
+    int rc = sort_device<uint64_t>(*C, CodecF64{d, d}, CodecF64{d, d}, n, st, use_learned(flags));
     if (rc) return rc;
     if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
     return finish_call(guard_, st, flags, host);
@@ -75,7 +75,7 @@ int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream) 
         S512_CUDA_TRY(cudaMemcpyAsync(dk, keys, n * sizeof(int), cudaMemcpyHostToDevice, st));
         S512_CUDA_TRY(cudaMemcpyAsync(dv, values, n * sizeof(int), cudaMemcpyHostToDevice, st));
     }
-    int rc = sort_device<uint64_t>(*C, CodecKV{dk, dv, dk, dv}, CodecKV{dk, dv, dk, dv}, n, st);
+    int rc = sort_device<uint64_t>(*C, CodecKV{dk, dv, dk, dv}, CodecKV{dk, dv, dk, dv}, n, st, use_learned(flags));
     if (rc) return rc;
     if (host) {
         S512_CUDA_TRY(cudaMemcpyAsync(keys, dk, n * sizeof(int), cudaMemcpyDeviceToHost, st));

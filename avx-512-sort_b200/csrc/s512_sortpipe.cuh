@@ -124,6 +124,8 @@ struct LevelCtl {
     uint32_t max_bucket;      // largest bucket seen this level
     uint32_t nonempty;        // non-empty buckets this level
     uint64_t level_keys;      // keys partitioned this level
+    uint32_t learned_used;    // segments routed by their learned model
+    uint32_t plain_used;      // segments routed by the splitter tree
 };
 
 // ===========================================================================
@@ -302,6 +304,12 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
     return range_b[j];
 }
 
+}  // namespace s512
+
+#include "s512_learned.cuh"
+
+namespace s512 {
+
 // ===========================================================================
 // 4. The partition pass (persistent; tiles claimed in order)
 //
@@ -319,6 +327,7 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
 // read with plain loads instead (a.tma == 0).
 
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
+constexpr int CLAIM_GROUP = 4; // consecutive tiles a block claims at once (one table load per group)
 constexpr int LOOKBACK_W = 8;  // predecessor statuses read per look-back step
 
 template <typename K>
@@ -335,6 +344,7 @@ struct PartArgs {
     const uint32_t* ntiles_dev;   // tile count written by prepare_level_kernel
     int tma;                      // tiles arrive by bulk copy
     uint32_t* chain;              // per segment: look-back positions handed out so far (zeroed)
+    const LearnedSet<K>* learned; // per segment learned model (nullptr: splitters only)
 };
 
 template <typename K, int THREADS, int IPT>
@@ -356,7 +366,8 @@ struct PartSmem {
     uint8_t ovf[NB];
     uint32_t eq_mask[NB / 32];
     uint64_t mbar[2];
-    uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos;
+    uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos, use_learned;
+    LearnedSet<K> L;
 };
 
 template <typename K, typename InCodec, int THREADS, int IPT>
@@ -413,9 +424,19 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
     };
 
     uint32_t claim_after = 0;  // thread 0: the tile claimed for two iterations ahead
+    // thread 0 claims CLAIM_GROUP consecutive tiles at a time, so that a block
+    // works through a run of one segment before it loads another's tables
+    uint32_t grp_next = 0, grp_end = 0;
+    auto claim = [&]() -> uint32_t {
+        if (grp_next == grp_end) {
+            grp_next = atomicAdd(&a.ctl->tile_counter, (uint32_t)CLAIM_GROUP);
+            grp_end = grp_next + CLAIM_GROUP;
+        }
+        return grp_next++;
+    };
     if (tid == 0) {
-        const uint32_t t0 = atomicAdd(&a.ctl->tile_counter, 1u);
-        const uint32_t t1 = atomicAdd(&a.ctl->tile_counter, 1u);
+        const uint32_t t0 = claim();
+        const uint32_t t1 = claim();
         sm.tile_cur = t0;
         sm.tile_next = t1;
         if (a.tma && t0 < ntiles) issue(t0, 0);
@@ -433,25 +454,39 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         uint32_t my_pos = 0;  // thread 0: look-back position of tile t (stored before the rank barrier)
         if (tid == 0) {
             if (a.tma && tn < ntiles) issue(tn, b ^ 1);
-            claim_after = atomicAdd(&a.ctl->tile_counter, 1u);  // consumed at the end of the iteration
+            claim_after = claim();  // consumed at the end of the iteration
             my_pos = atomicAdd(&a.chain[seg], 1u);
         }
         const SegDesc sd = a.segs[seg];
         if (seg != cached_seg) {
-            const SplitSet<K>& ss = a.splits[seg];
-            for (int i = tid; i < NB; i += THREADS) {
-                sm.tree[i] = ss.tree[i];
-                sm.uniq[i] = ss.uniq[i];
-                sm.region_off[i] = ss.region_off[i];
-                sm.region_cap[i] = ss.region_cap[i];
-                sm.range_b[i] = ss.range_b[i];
-                sm.eq_b[i] = ss.eq_b[i];
+            const bool use_learned = a.learned && a.learned[seg].ok;
+            if (use_learned) {
+                const LearnedSet<K>& ls = a.learned[seg];
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(&ls);
+                uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.L);
+                for (uint32_t i = tid; i < sizeof(LearnedSet<K>) / 4; i += THREADS) dst[i] = src[i];
+                for (int i = tid; i < NB; i += THREADS) {
+                    sm.region_off[i] = ls.region_off[i];
+                    sm.region_cap[i] = ls.region_cap[i];
+                }
+                if (tid == 0) sm.nbk = ls.nbuckets;
+            } else {
+                const SplitSet<K>& ss = a.splits[seg];
+                for (int i = tid; i < NB; i += THREADS) {
+                    sm.tree[i] = ss.tree[i];
+                    sm.uniq[i] = ss.uniq[i];
+                    sm.region_off[i] = ss.region_off[i];
+                    sm.region_cap[i] = ss.region_cap[i];
+                    sm.range_b[i] = ss.range_b[i];
+                    sm.eq_b[i] = ss.eq_b[i];
+                }
+                if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
+                if (tid == 0) {
+                    sm.has_eq = ss.has_eq;
+                    sm.nbk = ss.nbuckets;
+                }
             }
-            if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
-            if (tid == 0) {
-                sm.has_eq = ss.has_eq;
-                sm.nbk = ss.nbuckets;
-            }
+            if (tid == 0) sm.use_learned = use_learned ? 1u : 0u;
             cached_seg = seg;
         }
         const uint32_t ti = t - sd.tile_start;
@@ -467,6 +502,7 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         }
         __syncthreads();  // split set in shared memory
         const bool has_eq = sm.has_eq != 0;
+        const bool learned = sm.use_learned != 0;
 
         // keys: striped element r*THREADS + tid, from the bulk-copied tile
         // (tail elements past the copied bytes from global memory)
@@ -484,8 +520,9 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         for (int r = 0; r < IPT; ++r) {
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
             // lanes past the end of the tile carry the out-of-range bucket NB
-            bks[r] = idx < cnt ? find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask)
-                               : (uint32_t)NB;
+            if (idx >= cnt) bks[r] = (uint32_t)NB;
+            else if (learned) bks[r] = learned_bucket<K>(sm.L, key[r]);
+            else bks[r] = find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask);
         }
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
@@ -680,6 +717,7 @@ template <typename K>
 struct PlanArgs {
     const SegDesc* segs;
     const SplitSet<K>* splits;
+    const LearnedSet<K>* learned;       // used for segments whose model was accepted
     const uint64_t* bucket_counts;
     const K* level_out;                 // the level's output buffer
     LeafItem<K>* items[NCLASS + 1];     // per class, plus the copy list
@@ -696,17 +734,21 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
     const uint32_t s = blockIdx.x;
     if (s >= nsegs) return;
     const SegDesc sd = a.segs[s];
-    const SplitSet<K>& ss = a.splits[s];
+    const bool use_learned = a.learned && a.learned[s].ok;
+    const uint32_t nbk = use_learned ? a.learned[s].nbuckets : a.splits[s].nbuckets;
+    const uint64_t* region_off = use_learned ? a.learned[s].region_off : a.splits[s].region_off;
+    const uint32_t* bucket_eq = use_learned ? a.learned[s].bucket_eq : a.splits[s].bucket_eq;
     const int b = threadIdx.x;
-    const uint64_t c = (b < (int)ss.nbuckets) ? a.bucket_counts[(size_t)s * NB + b] : 0ull;
+    if (b == 0) atomicAdd(use_learned ? &a.ctl->learned_used : &a.ctl->plain_used, 1u);
+    const uint64_t c = (b < (int)nbk) ? a.bucket_counts[(size_t)s * NB + b] : 0ull;
     const uint64_t excl = block_exclusive_scan_first<NB, uint64_t>(c, wtot64, (uint64_t*)nullptr);
     if (c == 0) return;
     atomicMax(&a.ctl->max_bucket, (uint32_t)(c > 0xFFFFFFFFull ? 0xFFFFFFFFull : c));
     atomicAdd(&a.ctl->nonempty, 1u);
     atomicAdd((unsigned long long*)&a.ctl->level_keys, (unsigned long long)c);
-    const K* src = a.level_out + sd.out_base + ss.region_off[b];
+    const K* src = a.level_out + sd.out_base + region_off[b];
     const uint64_t dst = sd.final_off + excl;
-    const bool is_eq = (ss.bucket_eq[b >> 5] >> (b & 31)) & 1u;
+    const bool is_eq = (bucket_eq[b >> 5] >> (b & 31)) & 1u;
     if (is_eq || c == 1) {
         for (uint64_t o = 0; o < c; o += COPY_CHUNK) {
             const uint32_t slot = atomicAdd(&a.ctl->n_items[CLS_COPY], 1u);
@@ -738,7 +780,7 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
         const uint32_t slot = atomicAdd(&a.ctl->n_next, 1u);
         if (slot < a.next_cap) {
             SegDesc n;
-            n.in_off = sd.out_base + ss.region_off[b];
+            n.in_off = sd.out_base + region_off[b];
             n.count = c;
             n.final_off = dst;
             n.out_base = 0;

@@ -46,6 +46,7 @@ EXPORTS = (
     "s512_merge_i32", "s512_merge_f64", "s512_sort_omp_merge_i32", "s512_sort_omp_merge_f64",
     "s512_segsort_i32", "s512_segsort_f64", "s512_segsort_kv_i32", "s512_segsort_tune",
     "s512_segsort_plan_create", "s512_segsort_plan_launch", "s512_segsort_plan_destroy",
+    "s512_learned_root_grad", "s512_learned_fit",
 )
 
 DTYPE_I32, DTYPE_F64, DTYPE_KV_I32 = 0, 1, 2
@@ -144,6 +145,9 @@ def lib() -> ctypes.CDLL:
     L.s512_segsort_plan_create.argtypes = [ctypes.POINTER(vp), ci, vp, vp, vp, sz, vp]
     L.s512_segsort_plan_launch.argtypes = [vp, vp]
     L.s512_segsort_plan_destroy.argtypes = [vp]
+    L.s512_learned_root_grad.argtypes = [ci, vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float), vp]
+    L.s512_learned_fit.argtypes = [ci, vp, ctypes.c_uint32, ctypes.c_uint64, vp, vp, vp]
     _lib = L
     return L
 

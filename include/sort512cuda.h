@@ -180,6 +180,28 @@ S512_API int s512_segsort_plan_create(s512_segsort_plan** plan, int dtype, void*
 S512_API int s512_segsort_plan_launch(s512_segsort_plan* plan, void* stream);
 S512_API int s512_segsort_plan_destroy(s512_segsort_plan* plan);
 
+/* --- Learned splitters (no counterpart in the reference; S512_SPLIT_LEARNED).
+ *     Checking entry points of the model.  Keys are "encoded" keys: uint32
+ *     (int32 ^ 0x80000000) or uint64 (IEEE total-order bits of a double, or
+ *     (key,value) packed), ascending, in device memory.
+ *     s512_learned_root_grad: loss and dL/dtheta of the root piecewise-linear
+ *     CDF (64 pieces, slopes theta^2) for the given theta (host, 64 floats).
+ *     s512_learned_fit: fit the whole model to a sorted sample of a segment of
+ *     seg_count keys, as a partition level does (m must be the sample size the
+ *     library draws for that segment); optional per-bucket sample histogram. */
+#define S512_LEARNED_ROOT_PIECES 64
+typedef struct s512_learned_report {
+    float loss_init;      /* root loss at its histogram initialisation */
+    float loss_root;      /* root loss after training */
+    float loss_final;     /* loss of root + leaves */
+    float max_over_mean;  /* largest bucket / mean bucket, sample counts */
+    uint32_t nbuckets, nmodel, ok, pad_;
+} s512_learned_report;
+S512_API int s512_learned_root_grad(int key_bytes, const void* d_sorted_keys, uint32_t m, const float* theta,
+                                    float* loss, float* grad, void* stream);
+S512_API int s512_learned_fit(int key_bytes, const void* d_sorted_keys, uint32_t m, uint64_t seg_count,
+                              uint32_t* d_bucket_hist, s512_learned_report* report, void* stream);
+
 /* --- Sort512::popcount(__mmask16)   sort512.hpp:5714-5725 */
 S512_API int s512_popcount(unsigned mask);
 

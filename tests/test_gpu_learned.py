@@ -1,0 +1,133 @@
+"""Learned splitters on the GPU: the hand-written backward pass against the CPU
+oracle, the fit, and bit-exact sorts with the model routing keys (the model
+only decides bucket balance, never the result)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import learned_oracle as lo
+
+pytestmark = pytest.mark.gpu
+
+
+class Report(ctypes.Structure):
+    _fields_ = [("loss_init", ctypes.c_float), ("loss_root", ctypes.c_float), ("loss_final", ctypes.c_float),
+                ("max_over_mean", ctypes.c_float), ("nbuckets", ctypes.c_uint32), ("nmodel", ctypes.c_uint32),
+                ("ok", ctypes.c_uint32), ("pad_", ctypes.c_uint32)]
+
+
+def _keys(kind, m):
+    import workloads
+    if kind == "lognormal":
+        return np.sort(lo.encode_f64(workloads.lognormal_np(m, 5))), 8
+    if kind == "gauss_mix":
+        return np.sort(lo.encode_f64(workloads.gauss_mix_np(m, 6))), 8
+    if kind == "zipf":
+        return np.sort(lo.encode_i32(workloads.zipf_i32_np(m, seed=7))), 4
+    return np.sort(lo.encode_i32(workloads.uniform_i32_np(m, 8))), 4
+
+
+@pytest.mark.parametrize("kind", ["uniform", "zipf", "lognormal", "gauss_mix"])
+def test_root_gradient_matches_oracle(kind, s512, cuda):
+    import torch
+    keys, kb = _keys(kind, 16384)
+    d = torch.from_numpy(keys.view(np.int32 if kb == 4 else np.int64)).to(cuda)
+    theta = (lo.root_init_theta(keys) * (1.0 + 0.2 * np.cos(np.arange(lo.R)))).astype(np.float32)
+    loss = ctypes.c_float(0)
+    grad = (ctypes.c_float * lo.R)()
+    rc = s512.lib().s512_learned_root_grad(kb, ctypes.c_void_p(d.data_ptr()), len(keys),
+                                           theta.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                           ctypes.byref(loss), grad, None)
+    assert rc == 0
+    ref_loss, ref_grad = lo.root_loss_grad(keys, theta.astype(np.float64))
+    g = np.array(grad[:])
+    assert abs(loss.value - ref_loss) <= 1e-3 * max(ref_loss, 1e-9) + 1e-7
+    assert np.allclose(g, ref_grad, rtol=2e-3, atol=2e-3 * np.abs(ref_grad).max() + 1e-9)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "zipf", "lognormal", "gauss_mix"])
+def test_fit_trains_and_balances(kind, s512, cuda):
+    import torch
+    keys, kb = _keys(kind, 16384)
+    d = torch.from_numpy(keys.view(np.int32 if kb == 4 else np.int64)).to(cuda)
+    hist = torch.zeros(256, dtype=torch.int32, device=cuda)
+    rep = Report()
+    rc = s512.lib().s512_learned_fit(kb, ctypes.c_void_p(d.data_ptr()), len(keys), 1 << 26,
+                                     ctypes.c_void_p(hist.data_ptr()), ctypes.byref(rep), None)
+    assert rc == 0, s512.lib().s512_last_error_string()
+    # training never ends above its start; the leaves refine the root
+    assert rep.loss_root <= rep.loss_init * (1 + 1e-5) + 1e-12
+    assert rep.loss_final <= 2.0 * rep.loss_root + 1e-6
+    h = hist.cpu().numpy()
+    assert h.sum() == len(keys)
+    print(kind, "loss", rep.loss_init, rep.loss_root, rep.loss_final, "buckets", rep.nbuckets,
+          "max/mean", rep.max_over_mean, "ok", rep.ok)
+    if kind in ("uniform", "lognormal"):
+        assert rep.ok == 1
+
+
+@pytest.mark.parametrize("dist", ["uniform", "lognormal", "gauss_mix", "distinct256", "ascending", "descending"])
+def test_learned_sort_f64_exact(dist, s512, cuda):
+    import torch
+    import workloads
+    n = 1 << 22
+    t0 = workloads.double_dist_torch(dist, n, seed=11)
+    t = t0.clone()
+    s512.sort(t, flags=s512.SPLIT_LEARNED)
+    st = s512.stats()
+    assert torch.equal(t, torch.sort(t0).values), dist
+    assert st["fallbacks"] == 0 or st["learned_rejected"] > 0
+
+
+@pytest.mark.parametrize("dist", ["uniform", "zipf", "gauss_mix"])
+def test_learned_sort_i32_and_kv_exact(dist, s512, cuda):
+    import torch
+    import workloads
+    n = 1 << 22
+    if dist == "uniform":
+        k0 = workloads.uniform_i32_torch(n, 12)
+    elif dist == "zipf":
+        k0 = workloads.zipf_i32_torch(n, seed=12)
+    else:
+        k0 = workloads.gauss_mix_i32_torch(n, seed=12)
+    t = k0.clone()
+    s512.sort(t, flags=s512.SPLIT_LEARNED)
+    assert torch.equal(t, torch.sort(k0).values)
+    v0 = torch.arange(n, dtype=torch.int32, device=cuda)
+    k, v = k0.clone(), v0.clone()
+    s512.sort_kv(k, v, flags=s512.SPLIT_LEARNED)
+    assert torch.equal(k, torch.sort(k0).values) and torch.equal(k0[v.long()], k)
+
+
+def test_learned_versus_plain_routing(s512, cuda):
+    """What the trained model gains over the plain splitters on the same GPU:
+    the partition passes of both forms on skewed inputs (reported), with the
+    learned form used for every level it passed the balance check."""
+    import torch
+    import workloads
+    s512.set_config(collect_stats=1)
+    try:
+        rows = []
+        for name, mk in (("f64 lognormal", lambda: workloads.double_dist_torch("lognormal", 1 << 24, seed=3)),
+                         ("f64 gauss_mix", lambda: workloads.double_dist_torch("gauss_mix", 1 << 24, seed=3)),
+                         ("i32 zipf", lambda: workloads.zipf_i32_torch(1 << 24, seed=3))):
+            x0 = mk()
+            res = {}
+            for mode, flag in (("plain", s512.SPLIT_PLAIN), ("learned", s512.SPLIT_LEARNED)):
+                best = None
+                for _ in range(3):
+                    x = x0.clone()
+                    s512.sort(x, flags=flag)
+                    st = s512.stats()
+                    ms = sum(st["partition_ms"])
+                    best = ms if best is None else min(best, ms)
+                assert torch.equal(x, torch.sort(x0).values)
+                res[mode] = (best, st["learned_levels"], st["learned_rejected"], st["max_bucket_over_mean"])
+            rows.append((name, res))
+        for name, res in rows:
+            print(name, "partition ms plain %.3f learned %.3f (levels routed by the model %d, rejected %d)"
+                  % (res["plain"][0], res["learned"][0], res["learned"][1], res["learned"][2]))
+        assert any(res["learned"][1] > 0 for _, res in rows)
+    finally:
+        s512.set_config(collect_stats=0)
