@@ -162,6 +162,15 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
                                                            (float)config().max_imbalance);
         S512_LAUNCH_CHECK();
         S.kernel_launches += 1;
+        if (config().fault_inject & S512_FAULT_REJECT_MODEL) {
+            inject_reject_kernel<K><<<1, 256, 0, st>>>(lsets, nsegs);
+            S512_LAUNCH_CHECK();
+        }
+    }
+    const int fault = level == 0 ? config().fault_inject : 0;
+    if (fault & S512_FAULT_OVERFLOW) {
+        inject_overflow_kernel<K><<<1, NB, 0, st>>>(splits, lsets);
+        S512_LAUNCH_CHECK();
     }
     const int t1 = tm.mark();
 
@@ -179,6 +188,8 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     pa.tma = (L.aligned && codec_aligned(L.in)) ? 1 : 0;
     pa.chain = chain;
     pa.learned = lsets;
+    // the status array has one spare slot past the level's tiles, never written
+    pa.inject_slot = (fault & S512_FAULT_TIMEOUT) ? L.ntiles_bound : 0xFFFFFFFFu;
     auto pfn = partition_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
     const size_t psmem = sizeof(PartSmem<K, Shape::THREADS, Shape::IPT>);
     int pgrid = 0;
@@ -206,6 +217,10 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     S512_CUDA_TRY(cudaStreamSynchronize(st));
     S.kernel_launches += 1;
 
+    if (host_ctl->err & DEV_ERR_TIMEOUT) {
+        set_error("partition look-back wait timed out at level %d", level);
+        return S512_ERR_TIMEOUT;
+    }
     if (host_ctl->err & DEV_ERR_OVERFLOW) {
         // a bucket outgrew its sampled capacity: exact counts, exact regions,
         // redo with the splitters only
@@ -216,10 +231,11 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         const uint32_t ntiles = L.ntiles_dev ? host_ctl->ntiles_next : L.ntiles_host;
         (void)ntiles;
         S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
-        auto cfn = count_kernel<K, InCodec, 256, Shape::IPT>;
+        // same tile shape as the partition kernel: tiles are numbered for it
+        auto cfn = count_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
         int cgrid = 0;
-        S512_CUDA_TRY(launch_persistent(C, cfn, 256, 0, st, 0, &cgrid));
-        cfn<<<cgrid, 256, 0, st>>>(pa, L.in);
+        S512_CUDA_TRY(launch_persistent(C, cfn, Shape::THREADS, 0, st, 0, &cgrid));
+        cfn<<<cgrid, Shape::THREADS, 0, st>>>(pa, L.in);
         S512_LAUNCH_CHECK();
         exact_regions_kernel<K><<<nsegs, NB, 0, st>>>(splits, counts, nsegs);
         S512_LAUNCH_CHECK();

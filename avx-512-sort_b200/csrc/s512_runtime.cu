@@ -14,7 +14,7 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 
-static s512_config g_cfg = {S512_SPLIT_PLAIN, 0, 3.0, 0x5EEDull};
+static s512_config g_cfg = {S512_SPLIT_PLAIN, 0, 3.0, 0x5EEDull, 0};
 s512_config& config() { return g_cfg; }
 
 static thread_local s512_stats g_stats;
@@ -45,6 +45,10 @@ double PhaseTimer::ms(int a, int b) {
 // ---------------------------------------------------------------------------
 void* DevCtx::get(const char* name, size_t bytes) {
     if (bytes == 0) bytes = 256;
+    if (g_cfg.fault_inject & S512_FAULT_ALLOC) {
+        set_error("injected allocation failure (scratch '%s')", name);
+        return nullptr;
+    }
     auto it = bufs.find(name);
     if (it != bufs.end()) {
         if (it->second.second >= bytes) return it->second.first;

@@ -345,6 +345,8 @@ struct PartArgs {
     int tma;                      // tiles arrive by bulk copy
     uint32_t* chain;              // per segment: look-back positions handed out so far (zeroed)
     const LearnedSet<K>* learned; // per segment learned model (nullptr: splitters only)
+    uint32_t inject_slot;         // testing: chain position 1 of segment 0 waits on this
+                                  // never-written status slot (0xFFFFFFFF: off)
 };
 
 template <typename K, int THREADS, int IPT>
@@ -594,7 +596,17 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         if (tid < NB) {
             uint64_t prefix = 0;
             bool ok = data_ok;
-            if (pos > 0) {
+            if (pos == 1 && seg == 0 && a.inject_slot != 0xFFFFFFFFu) {
+                // injected failure: a predecessor that never publishes, waited
+                // for with a short bound
+                uint32_t spins = 0;
+                while (!(ld_status(&a.status[(size_t)a.inject_slot * NB + tid]) & (ST_INC | ST_AGG)) &&
+                       ++spins < 1024u)
+                    __nanosleep(100);
+                ok = false;
+                raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
+                st_status(&a.status[(size_t)slot * NB + tid], ST_INC | (unsigned long long)h);
+            } else if (pos > 0) {
                 // walk back through the chain LOOKBACK_W slots at a time (the
                 // loads of one window are in flight together); the segment's
                 // first slot always holds an inclusive count, so the walk ends
@@ -653,6 +665,22 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
     }
     // after an abort, let a copy still in flight land before the block exits
     if (a.tma && sm.abort && tid == 0 && sm.tile_cur < ntiles) mbar_wait_bounded(&sm.mbar[b], phase[b]);
+}
+
+// Testing: shrink every bucket capacity of segment 0 (forces an overflow).
+template <typename K>
+__global__ void inject_overflow_kernel(SplitSet<K>* splits, LearnedSet<K>* learned) {
+    const int b = threadIdx.x;
+    if (b < NB) {
+        if (splits[0].region_cap[b] > 16) splits[0].region_cap[b] = 16;
+        if (learned && learned[0].region_cap[b] > 16) learned[0].region_cap[b] = 16;
+    }
+}
+
+// Testing: reject every learned model of the level.
+template <typename K>
+__global__ void inject_reject_kernel(LearnedSet<K>* learned, uint32_t nsegs) {
+    for (uint32_t s = threadIdx.x; s < nsegs; s += blockDim.x) learned[s].ok = 0;
 }
 
 // Exact histogram of a level (the fallback after a capacity overflow).

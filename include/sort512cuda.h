@@ -67,7 +67,22 @@ typedef struct s512_config {
     int collect_stats;        /* 1: time every phase with CUDA events (s512_get_stats) */
     double max_imbalance;     /* learned model is rejected if max bucket > this x mean (default 3.0) */
     uint64_t seed;            /* sampling seed (default 0x5EED) */
+    int fault_inject;         /* testing only: S512_FAULT_* bits, 0 in normal use */
 } s512_config;
+
+/* Failure injection (tests of the library's own error paths; 0 by default).
+ * OVERFLOW shrinks the first level's bucket capacities so the partition pass
+ * overflows and the level is redone with exact counts; REJECT_MODEL rejects
+ * every learned model so the splitters route every level; ALLOC makes scratch
+ * allocation fail; TIMEOUT makes one tile of the first level wait on a status
+ * word that is never written, with a short bound, so the call returns
+ * S512_ERR_TIMEOUT while the device stays usable. */
+enum {
+    S512_FAULT_OVERFLOW = 1,
+    S512_FAULT_REJECT_MODEL = 2,
+    S512_FAULT_ALLOC = 4,
+    S512_FAULT_TIMEOUT = 8
+};
 
 /* per-call statistics of the last call on this host thread */
 #define S512_MAX_LEVELS 8

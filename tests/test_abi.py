@@ -40,7 +40,7 @@ def test_config_roundtrip_without_device(s512):
     s512.set_config(seed=1234)
     assert s512.get_config().seed == 1234
     s512.set_config(seed=0x5EED)
-    bad = s512.Config(99, 0, 3.0, 1)
+    bad = s512.Config(99, 0, 3.0, 1, 0)
     assert s512.lib().s512_set_config(ctypes.byref(bad)) == s512.S512_ERR_ARG
 
 
