@@ -339,6 +339,18 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def _timed(fn, stream):
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
 def run_extras(n, dev, stream):
     """One timed run per extra workload (reported beside the headline)."""
     import torch
@@ -347,21 +359,11 @@ def run_extras(n, dev, stream):
     import workloads
     out = {}
 
-    def timed(fn):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
-
     for dist in workloads.DOUBLE_DISTS:
         x = workloads.double_dist_torch(dist, n, seed=5, device=dev)
         s512.sort(x, flags=s512.ASYNC, stream=stream)  # warm
         x = workloads.double_dist_torch(dist, n, seed=6, device=dev)
-        ms = timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream))
+        ms = _timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream)
         ok = bool((x[1:] >= x[:-1]).all())
         st = s512.stats()
         out[f"f64_{dist}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "sorted": ok,
@@ -369,7 +371,7 @@ def run_extras(n, dev, stream):
         del x
     x = workloads.uniform_i32_torch(n, seed=8, device=dev)
     s512.sort(x.clone(), flags=s512.ASYNC, stream=stream)
-    ms = timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream))
+    ms = _timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream)
     out["i32_uniform"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
                           "sorted": bool((x[1:] >= x[:-1]).all())}
     del x
@@ -378,12 +380,189 @@ def run_extras(n, dev, stream):
                                                                                                          device=dev)
         v = torch.arange(n, dtype=torch.int32, device=dev)
         s512.sort_kv(k.clone(), v.clone(), flags=s512.ASYNC, stream=stream)
-        ms = timed(lambda: s512.sort_kv(k, v, flags=s512.ASYNC, stream=stream))
+        ms = _timed(lambda: s512.sort_kv(k, v, flags=s512.ASYNC, stream=stream), stream)
         out[f"kv_{kname}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
                               "sorted": bool((k[1:] >= k[:-1]).all())}
         del k, v
     torch.cuda.empty_cache()
+    out["int32_2p20_latency"] = extra_c1(dev, stream)
+    out["learned_vs_plain"] = extra_learned(dev, stream)
+    out["segmented_200k"] = extra_segsort(dev, stream)
+    torch.cuda.empty_cache()
     return out
+
+
+def extra_c1(dev, stream):
+    """int32, n = 2^20, uniform over the full range, seed 0: device latency,
+    the host-pointer call, exactness against the reference's output digest,
+    and the reference's single-core Sort on the same array."""
+    import hashlib
+
+    import numpy as np
+    import torch
+
+    import sort512cuda as s512
+    import workloads
+    n = 1 << 20
+    a = workloads.uniform_i32_np(n, 0)
+    d = torch.from_numpy(a).to(dev)
+    times = []
+    for _ in range(23):
+        x = d.clone()
+        torch.cuda.synchronize()
+        times.append(_timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream))
+    dev_ms = float(np.median(times[3:]))
+    h = a.copy()
+    t0 = time.perf_counter()
+    s512.sort(h)
+    host_ms = (time.perf_counter() - t0) * 1e3
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        want = json.load(f)["c1"]["sorted"]
+    exact = hashlib.sha256(h.tobytes()).hexdigest()[:32] == want
+    cpu_ms = None
+    try:
+        b = a.copy()
+        dt, kind, _ = cpu_reference_sort_array(b, "sort")
+        cpu_ms = dt * 1e3
+    except Exception:  # noqa: BLE001
+        kind = "unavailable"
+    return {"n": n, "device_ms_median": round(dev_ms, 4), "gkeys_s": round(n / dev_ms / 1e6, 3),
+            "host_pointer_call_ms": round(host_ms, 3), "exact_vs_reference_digest": exact,
+            "reference_sort_1core_ms": round(cpu_ms, 3) if cpu_ms else None, "reference_kind": kind}
+
+
+def cpu_reference_sort_array(a, fn="sort", threads=1):
+    sys.path.insert(0, ORACLE_DIR)
+    from oracle import REF_SO, Oracle, Reference, cpu_has_avx512
+    if os.path.exists(REF_SO) and cpu_has_avx512():
+        ref = Reference()
+        ref.set_threads(threads)
+        t0 = time.perf_counter()
+        ref.call(fn, a)
+        return time.perf_counter() - t0, "reference", threads
+    o = Oracle()
+    t0 = time.perf_counter()
+    o.sort(a)
+    return time.perf_counter() - t0, "port", 1
+
+
+def extra_learned(dev, stream):
+    """Learned vs sampled splitters on the same GPU: int32 n = 2^29 (Zipf 1.1
+    over 2^24 values; mixture of 8 Gaussians) and double n = 2^28 (lognormal
+    mu=0 sigma=2; mixture of 8 Gaussians): whole-sort and partition-pass
+    times, bucket imbalance, levels the model routed and models rejected."""
+    import torch
+
+    import sort512cuda as s512
+    import workloads
+    rows = {}
+    cases = (("i32_zipf_2p29", lambda: workloads.zipf_i32_torch(1 << 29, s=1.1, ranks=1 << 24, seed=21, device=dev)),
+             ("i32_gauss_mix_2p29", lambda: workloads.gauss_mix_i32_torch(1 << 29, seed=22, device=dev)),
+             ("f64_lognormal_2p28", lambda: workloads.double_dist_torch("lognormal", 1 << 28, seed=23, device=dev)),
+             ("f64_gauss_mix_2p28", lambda: workloads.double_dist_torch("gauss_mix", 1 << 28, seed=24, device=dev)))
+    for name, make in cases:
+        x0 = make()
+        n = x0.numel()
+        row = {"n": n}
+        for mode, flag in (("plain", s512.SPLIT_PLAIN), ("learned", s512.SPLIT_LEARNED)):
+            x = x0.clone()
+            s512.sort(x, flags=flag | s512.ASYNC, stream=stream)  # warm
+            x.copy_(x0)
+            ms = _timed(lambda: s512.sort(x, flags=flag | s512.ASYNC, stream=stream), stream)
+            st = s512.stats()
+            row[mode] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
+                         "partition_ms": round(sum(st["partition_ms"]), 3),
+                         "levels": st["levels"], "model_levels": st["learned_levels"],
+                         "models_rejected": st["learned_rejected"], "fallbacks": st["fallbacks"],
+                         "max_bucket_over_mean": [round(v, 2) for v in st["max_bucket_over_mean"]],
+                         "sorted": bool((x[1:] >= x[:-1]).all())}
+            del x
+        rows[name] = row
+        del x0
+        torch.cuda.empty_cache()
+    return rows
+
+
+def extra_segsort(dev, stream):
+    """200,000 segments, lognormal lengths (mu=5, sigma=1.5, clipped 1..65536):
+    int32 uniform, double U[0,1) and int32 key/value, one graph-captured
+    persistent launch (plus partition levels for segments above a block),
+    against a loop of single-array sorts over a sample of the segments and the
+    reference's loop (SmallSort16V / Sort) on the host for the same sample."""
+    import numpy as np
+    import torch
+
+    import sort512cuda as s512
+    import workloads
+    nseg = 200_000
+    lens = workloads.segment_lengths_np(nseg, 31)
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    total = int(off[-1])
+    d_off = torch.from_numpy(off.view(np.int64)).to(dev)
+    res = {"segments": nseg, "keys": total}
+    tuned = {}
+    for dt in (s512.DTYPE_I32, s512.DTYPE_F64, s512.DTYPE_KV_I32):
+        tuned[dt] = s512.segsort_tune(dt, d_off)[1]
+    for name, dt in (("i32", s512.DTYPE_I32), ("f64", s512.DTYPE_F64), ("kv_i32", s512.DTYPE_KV_I32)):
+        if dt == s512.DTYPE_F64:
+            keys0 = workloads.uniform01_torch(total, 32, dev)
+        else:
+            keys0 = workloads.uniform_i32_torch(total, 33, dev)
+        vals0 = torch.arange(total, dtype=torch.int32, device=dev) if dt == s512.DTYPE_KV_I32 else None
+        keys = keys0.clone()
+        vals = vals0.clone() if vals0 is not None else None
+        plan = s512.SegsortPlan(dt, keys, d_off, values=vals)
+        times = []
+        for rep in range(4):
+            keys.copy_(keys0)
+            if vals is not None:
+                vals.copy_(vals0)
+            times.append(_timed(lambda: plan.launch(stream), stream))
+        plan.close()
+        ms = float(np.median(times[1:]))
+        # a loop of single-array sorts over every 100th segment, scaled up
+        idx = list(range(0, nseg, 100))
+        sub = keys0.clone()
+        loop_ms = _timed(lambda: [s512.sort(sub[int(off[i]):int(off[i + 1])], flags=s512.ASYNC, stream=stream)
+                                  if dt != s512.DTYPE_KV_I32 else
+                                  s512.sort_kv(sub[int(off[i]):int(off[i + 1])],
+                                               vals0[int(off[i]):int(off[i + 1])].clone(), flags=s512.ASYNC,
+                                               stream=stream)
+                                  for i in idx], stream)
+        sample_keys = int(sum(int(off[i + 1] - off[i]) for i in idx))
+        loop_est_ms = loop_ms * total / max(sample_keys, 1)
+        ok = True
+        kh = keys.cpu().numpy()
+        for i in idx[::20]:
+            seg = kh[int(off[i]):int(off[i + 1])]
+            ok = ok and bool(np.all(seg[1:] >= seg[:-1]))
+        row = {"gkeys_s": round(total / ms / 1e6, 3), "ms": round(ms, 3), "launch_shape": tuned[dt],
+               "loop_of_sorts_est_ms": round(loop_est_ms, 1), "sorted_sample": ok}
+        # the reference's loop on the host for the same sample of segments
+        try:
+            sys.path.insert(0, ORACLE_DIR)
+            from oracle import REF_SO, Reference, cpu_has_avx512
+            if os.path.exists(REF_SO) and cpu_has_avx512():
+                ref = Reference()
+                ref.set_threads(1)
+                host = keys0.cpu().numpy()
+                hv = vals0.cpu().numpy() if vals0 is not None else None
+                lim = 256 if dt != s512.DTYPE_F64 else 128
+                t0 = time.perf_counter()
+                for i in idx:
+                    a = host[int(off[i]):int(off[i + 1])]
+                    if dt == s512.DTYPE_KV_I32:
+                        ref.call_kv("smallsort" if a.size <= lim else "sort", a, hv[int(off[i]):int(off[i + 1])])
+                    else:
+                        ref.call("smallsort" if a.size <= lim else "sort", a)
+                cpu_s = time.perf_counter() - t0
+                row["reference_loop_1core_est_ms"] = round(cpu_s * 1e3 * total / max(sample_keys, 1), 1)
+        except Exception as e:  # noqa: BLE001
+            row["reference_loop_error"] = str(e)[:120]
+        res[name] = row
+        del keys, keys0, vals, vals0, sub
+        torch.cuda.empty_cache()
+    return res
 
 
 def main():
