@@ -38,8 +38,8 @@ namespace s512 {
 constexpr int LR_ROOT = 64;
 constexpr int LR_LEAVES = 256;
 constexpr int LR_THREADS = 512;
-constexpr int LR_ITERS = 40;
-constexpr int LR_LEAF_ITERS = 20;
+constexpr int LR_ITERS = 16;
+constexpr int LR_LEAF_ITERS = 8;
 constexpr float LR_STEP = 0.02f;  // Adam step, relative to the parameters' scale
 
 template <typename K>
@@ -441,14 +441,13 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
         atomicMax(&max_s, c);
         atomicAdd(&nonempty_s, 1u);
     }
-    uint32_t eq_bit = 0;
-    if (tid < NB) {
-        // bucket tid is an "equal" bucket if it is base_id[r]+1 of a heavy model bucket
-        for (uint32_t r = 0; r < nmodel; ++r)
-            if (L.heavy_flag[r] && (uint32_t)L.base_id[r] + 1 == (uint32_t)tid) eq_bit = 1;
+    // the "equal" bucket of each heavy model bucket r is base_id[r] + 1
+    if (tid < NB / 32) L.bucket_eq[tid] = 0;
+    __syncthreads();
+    if (tid < (int)nmodel && L.heavy_flag[tid]) {
+        const uint32_t e = (uint32_t)L.base_id[tid] + 1;
+        atomicOr(&L.bucket_eq[e >> 5], 1u << (e & 31));
     }
-    const unsigned bal = __ballot_sync(0xFFFFFFFFu, eq_bit != 0);
-    if (tid < NB && (tid & 31) == 0) L.bucket_eq[tid >> 5] = bal;
     const double scale = (double)sd.count / (double)m;
     uint64_t cap = 0;
     if (tid < NB && (uint32_t)tid < L.nbuckets) {

@@ -42,7 +42,7 @@ static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint3
         case 1: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, st);
         case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, st);
         case 3: return launch_leaf_block<K, OutCodec, 512, 8>(C, items, n, out, st);
-        case 4: return launch_leaf_block<K, OutCodec, 1024, 8>(C, items, n, out, st);
+        case 4: return launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, st);
         case 5: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, st);
         case CLS_COPY: {
             auto fn = leaf_copy_kernel<K, OutCodec>;
@@ -81,7 +81,7 @@ static int sort_one_leaf(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaSt
         case 1: return launch_small_block<InCodec, OutCodec, 128, 8>(C, in, out, n, st);
         case 2: return launch_small_block<InCodec, OutCodec, 256, 8>(C, in, out, n, st);
         case 3: return launch_small_block<InCodec, OutCodec, 512, 8>(C, in, out, n, st);
-        case 4: return launch_small_block<InCodec, OutCodec, 1024, 8>(C, in, out, n, st);
+        case 4: return launch_small_block<InCodec, OutCodec, 512, 16>(C, in, out, n, st);
         default: return launch_small_block<InCodec, OutCodec, 1024, 16>(C, in, out, n, st);
     }
 }

@@ -448,10 +448,11 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
     int b = 0;
 
     while (true) {
+        // tile_cur / tile_next are rewritten by thread 0 only after the
+        // barriers below, so reading them needs no barrier of its own
         const uint32_t t = sm.tile_cur;
         const uint32_t tn = sm.tile_next;
         if (t >= ntiles || sm.abort) break;
-        __syncthreads();  // everyone has read tile_cur / tile_next
         const uint32_t seg = seg_of(t);
         uint32_t my_pos = 0;  // thread 0: look-back position of tile t (stored before the rank barrier)
         if (tid == 0) {
@@ -460,7 +461,8 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             my_pos = atomicAdd(&a.chain[seg], 1u);
         }
         const SegDesc sd = a.segs[seg];
-        if (seg != cached_seg) {
+        const bool new_seg = seg != cached_seg;
+        if (new_seg) {
             const bool use_learned = a.learned && a.learned[seg].ok;
             if (use_learned) {
                 const LearnedSet<K>& ls = a.learned[seg];
@@ -498,11 +500,13 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
         bool data_ok = true;
         if (a.tma) {
+            // every thread waits on the barrier itself: the bulk copy's data is
+            // then visible to it without a block barrier
             data_ok = mbar_wait_bounded(&sm.mbar[b], phase[b]);
             phase[b] ^= 1u;
             if (!data_ok) raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
         }
-        __syncthreads();  // split set in shared memory
+        if (new_seg) __syncthreads();  // the segment's tables in shared memory
         const bool has_eq = sm.has_eq != 0;
         const bool learned = sm.use_learned != 0;
 
