@@ -18,7 +18,7 @@ template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT
 template <typename K, typename OutCodec, int THREADS, int EPT>
 static int launch_leaf_block(DevCtx& C, const LeafItem<K>* items, uint32_t n, OutCodec out, cudaStream_t st) {
     auto fn = leaf_block_kernel<K, OutCodec, THREADS, EPT>;
-    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
+    const size_t smem = SlotSmem<K, THREADS, EPT>::bytes;
     int grid = 0;
     S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
     fn<<<grid, THREADS, smem, st>>>(items, n, out);
@@ -62,7 +62,7 @@ template <typename InCodec, typename OutCodec, int THREADS, int EPT>
 static int launch_small_block(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaStream_t st) {
     using K = typename InCodec::Key;
     auto fn = small_block_sort_kernel<InCodec, OutCodec, THREADS, EPT>;
-    const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
+    const size_t smem = SlotSmem<K, THREADS, EPT>::bytes;
     S512_CUDA_TRY(C.prepare((const void*)fn, smem));
     fn<<<1, THREADS, smem, st>>>(in, out, n);
     S512_LAUNCH_CHECK();

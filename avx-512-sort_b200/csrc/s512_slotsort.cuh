@@ -1,0 +1,219 @@
+// s512_slotsort.cuh -- one bucket sorted by distribution counting: keys are
+// dealt into value slots by a monotone linear map of their offset from the
+// bucket's minimum, the slots are laid out by an exclusive scan of their
+// counts, and every key finds its final place by ranking itself inside its
+// own (short) slot.
+//
+// A bucket that reaches the leaf stage holds the keys between two adjacent
+// quantile splitters, so its values are close to evenly spread over
+// [min, max]: with as many slots as the class has keys, a slot holds about
+// one key and the whole sort costs a few shared-memory operations per key,
+// where a comparison network costs one compare-exchange per key for every
+// stage.  When the spread is uneven (a cluster, a run of repeated values, an
+// outlier that stretches the range) the slot counts show it before any key
+// moves: if the largest slot exceeds SLOT_MAX_RUN keys, or the ranking work
+// (the sum of squared slot counts) exceeds SLOT_SUMSQ per key, the bucket is
+// sorted by the bitonic + merge-path block sort instead (s512_blocksort.cuh).
+//
+// Equal keys are identical encoded words (see s512_common.cuh), so placing
+// ties in any order gives the same output; the in-slot rank breaks ties by
+// shared-memory position only to make the ranks a permutation.
+#pragma once
+
+#include "s512_blocksort.cuh"
+
+namespace s512 {
+
+constexpr uint32_t SLOT_MAX_RUN = 32;  // largest slot ranked key by key
+constexpr uint32_t SLOT_SUMSQ = 4;     // ranking work allowed per key
+
+// Monotone map from a key in [lo, hi] to a slot in [0, nslots): the offset
+// x - lo is cut to its 32 leading significant bits (shift sh), then either
+// used as the slot itself (direct, when the cut range is below nslots) or
+// scaled by mul / 2^32 with mul = floor(nslots * 2^32 / (range + 1)), which
+// keeps the largest offset below nslots.
+template <typename K>
+struct SlotMap {
+    K lo;
+    uint32_t sh, mul, direct;
+    __device__ __forceinline__ uint32_t operator()(K x) const {
+        const uint32_t d = (uint32_t)((x - lo) >> sh);
+        return direct ? d : __umulhi(d, mul);
+    }
+};
+
+template <typename K>
+__device__ __forceinline__ SlotMap<K> make_slot_map(K lo, K hi, uint32_t nslots) {
+    SlotMap<K> f;
+    f.lo = lo;
+    const K range = hi - lo;
+    int nb;
+    if constexpr (sizeof(K) == 8) nb = 64 - __clzll((long long)range);
+    else nb = 32 - __clz((int)range);
+    f.sh = nb > 32 ? (uint32_t)(nb - 32) : 0u;
+    const uint32_t dr = (uint32_t)(range >> f.sh);
+    f.direct = dr < nslots ? 1u : 0u;
+    f.mul = f.direct ? 0u : (uint32_t)(((uint64_t)nslots << 32) / ((uint64_t)dr + 1));
+    return f;
+}
+
+// Per-warp partials of the block reductions.
+template <typename K>
+struct SlotRed {
+    K wlo[32], whi[32];
+    uint32_t wtot[32], wmax[32], wsq[32];
+};
+
+// Shared memory of block_slot_sort for a block of THREADS x IPT keys: the
+// key buffer (padded for the fallback block sort) followed by the counters.
+template <typename K, int THREADS, int IPT>
+struct SlotSmem {
+    static constexpr uint32_t S = (uint32_t)THREADS * IPT;
+    static constexpr size_t keys_bytes = ((size_t)padded_len(S) * sizeof(K) + 15) & ~(size_t)15;
+    static constexpr size_t bytes = keys_bytes + (size_t)S * sizeof(uint32_t);
+};
+
+// Sort the c <= THREADS*IPT keys load(0..c) into store(0..c).  `smem` holds
+// SlotSmem<K,THREADS,IPT>::bytes; `red` is the block's reduction scratch.
+// Every thread of the block must call it; it ends with a barrier, so the
+// caller may reuse the shared memory right after.  Returns true when the
+// bucket took the distribution-counting path.
+template <typename K, int THREADS, int IPT, typename Load, typename Store>
+__device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned char* smem, SlotRed<K>& red) {
+    constexpr uint32_t S = (uint32_t)THREADS * IPT;
+    constexpr int NW = THREADS / 32;
+    static_assert(IPT % 4 == 0, "counters are read four at a time");
+    K* s = reinterpret_cast<K*>(smem);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SlotSmem<K, THREADS, IPT>::keys_bytes);
+    const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
+
+    // 1. keys into registers (striped), bounds of the bucket, counters zeroed
+    K key[IPT];
+    K lo = KeyMax<K>::value, hi = K(0);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t i = (uint32_t)r * THREADS + tid;
+        if (i < c) {
+            key[r] = load(i);
+            lo = kmin(lo, key[r]);
+            hi = kmax(hi, key[r]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < IPT; r += 4)
+        *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = kmin(lo, shfl_xor(lo, d));
+        hi = kmax(hi, shfl_xor(hi, d));
+    }
+    if (lane == 0) {
+        red.wlo[warp] = lo;
+        red.whi[warp] = hi;
+    }
+    __syncthreads();
+    lo = lane < (unsigned)NW ? red.wlo[lane] : KeyMax<K>::value;
+    hi = lane < (unsigned)NW ? red.whi[lane] : K(0);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = kmin(lo, shfl_xor(lo, d));
+        hi = kmax(hi, shfl_xor(hi, d));
+    }
+
+    if (lo == hi) {  // every key equal: already in order
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + tid;
+            if (i < c) store(i, key[r]);
+        }
+        __syncthreads();
+        return true;
+    }
+
+    // 2. slot counts
+    const SlotMap<K> f = make_slot_map<K>(lo, hi, S);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t i = (uint32_t)r * THREADS + tid;
+        if (i < c) atomicAdd(&ctr[f(key[r])], 1u);
+    }
+    __syncthreads();
+
+    // 3. exclusive scan of the counts (IPT consecutive counters per thread),
+    //    with the largest count and the sum of squared counts
+    uint32_t sum = 0, mx = 0, sq = 0;
+#pragma unroll
+    for (int r = 0; r < IPT; r += 4) {
+        const uint4 q = *reinterpret_cast<const uint4*>(&ctr[tid * IPT + r]);
+        sum += q.x + q.y + q.z + q.w;
+        mx = max(max(mx, max(q.x, q.y)), max(q.z, q.w));
+        sq += q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
+    }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
+        sq += __shfl_xor_sync(0xFFFFFFFFu, sq, d);
+    }
+    if (lane == 0) {
+        red.wmax[warp] = mx;
+        red.wsq[warp] = sq;
+    }
+    const uint32_t base = block_exclusive_scan_first<THREADS, uint32_t>(sum, red.wtot, (uint32_t*)nullptr);
+    // (the scan's barriers publish wmax / wsq)
+    mx = lane < (unsigned)NW ? red.wmax[lane] : 0u;
+    sq = lane < (unsigned)NW ? red.wsq[lane] : 0u;
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
+        sq += __shfl_xor_sync(0xFFFFFFFFu, sq, d);
+    }
+    const bool even = mx <= SLOT_MAX_RUN && sq <= SLOT_SUMSQ * c;
+
+    if (even) {
+        // counts -> slot starts (the counters are read again rather than kept
+        // in registers across the scan)
+        uint32_t run = base;
+#pragma unroll
+        for (int r = 0; r < IPT; r += 4) {
+            uint4 q = *reinterpret_cast<const uint4*>(&ctr[tid * IPT + r]);
+            const uint32_t s0 = run, s1 = s0 + q.x, s2 = s1 + q.y, s3 = s2 + q.z;
+            run = s3 + q.w;
+            q = make_uint4(s0, s1, s2, s3);
+            *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = q;
+        }
+        __syncthreads();
+        // 4. deal the keys into their slots; afterwards ctr[j] is the end of slot j
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + tid;
+            if (i < c) s[atomicAdd(&ctr[f(key[r])], 1u)] = key[r];
+        }
+        __syncthreads();
+        // 5. rank each key inside its slot and write it to its final place
+        for (uint32_t p = tid; p < c; p += THREADS) {
+            const K x = s[p];
+            const uint32_t j = f(x);
+            const uint32_t a = j ? ctr[j - 1] : 0u;
+            const uint32_t e = ctr[j];
+            uint32_t rank = a;
+            for (uint32_t q = a; q < e; ++q) {
+                const K y = s[q];
+                rank += (y < x || (y == x && q < p)) ? 1u : 0u;
+            }
+            store(rank, x);
+        }
+    } else {
+        // uneven spread: bitonic leaves + merge path on the same keys
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + tid;
+            if (i < c) s[pidx(i)] = key[r];
+        }
+        block_merge_sort<K, THREADS, IPT>(s, c);
+        for (uint32_t i = tid; i < c; i += THREADS) store(i, s[pidx(i)]);
+    }
+    __syncthreads();
+    return even;
+}
+
+}  // namespace s512

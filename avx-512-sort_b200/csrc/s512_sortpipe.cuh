@@ -25,7 +25,7 @@
 //     next partition level.
 #pragma once
 
-#include "s512_blocksort.cuh"
+#include "s512_slotsort.cuh"
 
 namespace s512 {
 
@@ -899,18 +899,21 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
     }
 }
 
-// One block per bucket of at most THREADS*EPT keys.
+// One block per bucket of at most THREADS*EPT keys: distribution counting
+// into value slots, or bitonic leaves + merge path when the slots come out
+// uneven (s512_slotsort.cuh).
 template <typename K, typename OutCodec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS) leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
                                                              OutCodec out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* s = reinterpret_cast<K*>(smem_raw);
+    __shared__ SlotRed<K> red;
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const LeafItem<K> item = items[it];
-        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) s[pidx(i)] = item.src[i];
-        block_merge_sort<K, THREADS, EPT>(s, item.count);
-        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) out.store(item.dst + i, s[pidx(i)]);
-        __syncthreads();
+        const K* __restrict__ src = item.src;
+        const size_t dst = item.dst;
+        block_slot_sort<K, THREADS, EPT>([&](uint32_t i) { return src[i]; },
+                                         [&](uint32_t i, K x) { out.store(dst + i, x); }, item.count, smem_raw,
+                                         red);
     }
 }
 
@@ -946,13 +949,11 @@ __global__ void __launch_bounds__(32) small_warp_sort_kernel(InCodec in, OutCode
 }
 
 template <typename InCodec, typename OutCodec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS) small_block_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) small_block_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
     using K = typename InCodec::Key;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* s = reinterpret_cast<K*>(smem_raw);
-    for (uint32_t i = threadIdx.x; i < n; i += THREADS) s[pidx(i)] = in.load(i);
-    block_merge_sort<K, THREADS, EPT>(s, n);
-    for (uint32_t i = threadIdx.x; i < n; i += THREADS) out.store(i, s[pidx(i)]);
+    __shared__ SlotRed<K> red;
+    block_slot_sort<K, THREADS, EPT>([&](uint32_t i) { return in.load(i); },
+                                     [&](uint32_t i, K x) { out.store(i, x); }, n, smem_raw, red);
 }
-
 }  // namespace s512
