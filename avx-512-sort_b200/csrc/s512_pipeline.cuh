@@ -15,20 +15,35 @@ template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT
 // ---------------------------------------------------------------------------
 // leaf launches per class
 
+// Slot sort of a class's buckets, then the block sort of those it found
+// uneven (the second launch reads the count on the device and exits at once
+// when there are none).
 template <typename K, typename OutCodec, int THREADS, int EPT>
-static int launch_leaf_block(DevCtx& C, const LeafItem<K>* items, uint32_t n, OutCodec out, cudaStream_t st) {
-    auto fn = leaf_block_kernel<K, OutCodec, THREADS, EPT>;
-    const size_t smem = SlotSmem<K, THREADS, EPT>::bytes;
-    int grid = 0;
-    S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
-    fn<<<grid, THREADS, smem, st>>>(items, n, out);
-    S512_LAUNCH_CHECK();
+static int launch_leaf_block(DevCtx& C, const LeafItem<K>* items, uint32_t n, OutCodec out, LeafItem<K>* uneven,
+                             uint32_t* n_uneven, cudaStream_t st) {
+    {
+        auto fn = leaf_block_kernel<K, OutCodec, THREADS, EPT>;
+        const size_t smem = SlotSmem<K, THREADS, EPT>::bytes;
+        int grid = 0;
+        S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
+        fn<<<grid, THREADS, smem, st>>>(items, n, out, uneven, n_uneven);
+        S512_LAUNCH_CHECK();
+    }
+    {
+        auto fn = leaf_merge_kernel<K, OutCodec, THREADS, EPT>;
+        const size_t smem = (size_t)padded_len(THREADS * EPT) * sizeof(K);
+        int grid = 0;
+        S512_CUDA_TRY(launch_persistent(C, fn, THREADS, smem, st, (int)n, &grid));
+        fn<<<grid, THREADS, smem, st>>>(uneven, n_uneven, out);
+        S512_LAUNCH_CHECK();
+    }
     return S512_OK;
 }
 
+// Launch the leaf kernels of one class.  `uneven` has room for n items.
 template <typename K, typename OutCodec>
 static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint32_t n, OutCodec out,
-                             cudaStream_t st) {
+                             LeafItem<K>* uneven, uint32_t* n_uneven, cudaStream_t st) {
     if (n == 0) return S512_OK;
     switch (cls) {
         case 0: {
@@ -39,11 +54,11 @@ static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint3
             S512_LAUNCH_CHECK();
             return S512_OK;
         }
-        case 1: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, st);
-        case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, st);
-        case 3: return launch_leaf_block<K, OutCodec, 512, 8>(C, items, n, out, st);
-        case 4: return launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, st);
-        case 5: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, st);
+        case 1: return launch_leaf_block<K, OutCodec, 128, 8>(C, items, n, out, uneven, n_uneven, st);
+        case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, uneven, n_uneven, st);
+        case 3: return launch_leaf_block<K, OutCodec, 256, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 4: return launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 5: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, uneven, n_uneven, st);
         case CLS_COPY: {
             auto fn = leaf_copy_kernel<K, OutCodec>;
             int grid = 0;
@@ -262,11 +277,18 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
 
     // leaves of this level
     const int t3 = tm.mark();
+    size_t n_block_items = 0;
+    for (int c = 1; c < NCLASS; ++c) n_block_items += host_ctl->n_items[c];
+    LeafItem<K>* uneven =
+        n_block_items ? (LeafItem<K>*)C.get("uneven", n_block_items * sizeof(LeafItem<K>)) : nullptr;
+    if (n_block_items && !uneven) return S512_ERR_ALLOC;
     for (int c = 0; c <= NCLASS; ++c) {
         if (host_ctl->n_items[c] == 0) continue;
-        rc = launch_leaf_class<K, UserOut>(C, c, items[c], host_ctl->n_items[c], uout, st);
+        rc = launch_leaf_class<K, UserOut>(C, c, items[c], host_ctl->n_items[c], uout, uneven,
+                                           c < NCLASS ? &ctl->n_uneven[c] : nullptr, st);
         if (rc) return rc;
-        S.kernel_launches += 1;
+        S.kernel_launches += (c >= 1 && c < NCLASS) ? 2 : 1;
+        if (c >= 1 && c < NCLASS) uneven += host_ctl->n_items[c];
     }
     const int t4 = tm.mark();
 

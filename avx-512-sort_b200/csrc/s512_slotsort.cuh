@@ -73,13 +73,22 @@ struct SlotSmem {
     static constexpr size_t bytes = keys_bytes + (size_t)S * sizeof(uint32_t);
 };
 
-// Sort the c <= THREADS*IPT keys load(0..c) into store(0..c).  `smem` holds
-// SlotSmem<K,THREADS,IPT>::bytes; `red` is the block's reduction scratch.
-// Every thread of the block must call it; it ends with a barrier, so the
-// caller may reuse the shared memory right after.  Returns true when the
-// bucket took the distribution-counting path.
-template <typename K, int THREADS, int IPT, typename Load, typename Store>
-__device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned char* smem, SlotRed<K>& red) {
+// Sort the c <= THREADS*IPT keys held striped in key[] (element
+// r*THREADS + tid in key[r]; entries past c are ignored) into store(0..c).
+// `smem` holds SlotSmem<K,THREADS,IPT>::bytes; `red` is the block's reduction
+// scratch.  refill() is called exactly once, as soon as key[] is no longer
+// needed, so that the caller can start loading the next bucket into it while
+// this one is ranked and written.  Every thread of the block must call it; it
+// ends with a barrier, so the caller may reuse the shared memory right after.
+// Returns true when the bucket took the distribution-counting path.
+//
+// An uneven bucket is sorted here by the block sort when INLINE_FALLBACK is
+// set; otherwise thread 0 calls uneven() (which hands the bucket to a
+// separate launch) and nothing is written.  Keeping the block sort out of
+// the kernel keeps the slot path's register budget for the keys.
+template <typename K, int THREADS, int IPT, bool INLINE_FALLBACK, typename Store, typename Refill, typename Uneven>
+__device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill refill, Uneven uneven,
+                                unsigned char* smem, SlotRed<K>& red) {
     constexpr uint32_t S = (uint32_t)THREADS * IPT;
     constexpr int NW = THREADS / 32;
     static_assert(IPT % 4 == 0, "counters are read four at a time");
@@ -87,14 +96,11 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
     uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SlotSmem<K, THREADS, IPT>::keys_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
-    // 1. keys into registers (striped), bounds of the bucket, counters zeroed
-    K key[IPT];
+    // 1. bounds of the bucket; counters zeroed
     K lo = KeyMax<K>::value, hi = K(0);
 #pragma unroll
     for (int r = 0; r < IPT; ++r) {
-        const uint32_t i = (uint32_t)r * THREADS + tid;
-        if (i < c) {
-            key[r] = load(i);
+        if ((uint32_t)r * THREADS + tid < c) {
             lo = kmin(lo, key[r]);
             hi = kmax(hi, key[r]);
         }
@@ -126,6 +132,7 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
             const uint32_t i = (uint32_t)r * THREADS + tid;
             if (i < c) store(i, key[r]);
         }
+        refill();
         __syncthreads();
         return true;
     }
@@ -134,13 +141,13 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
     const SlotMap<K> f = make_slot_map<K>(lo, hi, S);
 #pragma unroll
     for (int r = 0; r < IPT; ++r) {
-        const uint32_t i = (uint32_t)r * THREADS + tid;
-        if (i < c) atomicAdd(&ctr[f(key[r])], 1u);
+        if ((uint32_t)r * THREADS + tid < c) atomicAdd(&ctr[f(key[r])], 1u);
     }
     __syncthreads();
 
-    // 3. exclusive scan of the counts (IPT consecutive counters per thread),
-    //    with the largest count and the sum of squared counts
+    // 3. exclusive scan of the counts (IPT consecutive counters per thread)
+    //    with the largest count and the sum of squared counts; one barrier:
+    //    every warp scans the per-warp totals itself
     uint32_t sum = 0, mx = 0, sq = 0;
 #pragma unroll
     for (int r = 0; r < IPT; r += 4) {
@@ -149,21 +156,29 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
         mx = max(max(mx, max(q.x, q.y)), max(q.z, q.w));
         sq += q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w;
     }
+    uint32_t inc = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+        if (lane >= (unsigned)d) inc += o;
+    }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
         sq += __shfl_xor_sync(0xFFFFFFFFu, sq, d);
     }
+    if (lane == 31) red.wtot[warp] = inc;
     if (lane == 0) {
         red.wmax[warp] = mx;
         red.wsq[warp] = sq;
     }
-    const uint32_t base = block_exclusive_scan_first<THREADS, uint32_t>(sum, red.wtot, (uint32_t*)nullptr);
-    // (the scan's barriers publish wmax / wsq)
+    __syncthreads();
+    uint32_t before = (lane < warp) ? red.wtot[lane] : 0u;
     mx = lane < (unsigned)NW ? red.wmax[lane] : 0u;
     sq = lane < (unsigned)NW ? red.wsq[lane] : 0u;
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
+        before += __shfl_xor_sync(0xFFFFFFFFu, before, d);
         mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
         sq += __shfl_xor_sync(0xFFFFFFFFu, sq, d);
     }
@@ -171,8 +186,8 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
 
     if (even) {
         // counts -> slot starts (the counters are read again rather than kept
-        // in registers across the scan)
-        uint32_t run = base;
+        // in registers across the barrier)
+        uint32_t run = before + inc - sum;
 #pragma unroll
         for (int r = 0; r < IPT; r += 4) {
             uint4 q = *reinterpret_cast<const uint4*>(&ctr[tid * IPT + r]);
@@ -185,9 +200,9 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
         // 4. deal the keys into their slots; afterwards ctr[j] is the end of slot j
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            const uint32_t i = (uint32_t)r * THREADS + tid;
-            if (i < c) s[atomicAdd(&ctr[f(key[r])], 1u)] = key[r];
+            if ((uint32_t)r * THREADS + tid < c) s[atomicAdd(&ctr[f(key[r])], 1u)] = key[r];
         }
+        refill();
         __syncthreads();
         // 5. rank each key inside its slot and write it to its final place
         for (uint32_t p = tid; p < c; p += THREADS) {
@@ -202,7 +217,7 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
             }
             store(rank, x);
         }
-    } else {
+    } else if constexpr (INLINE_FALLBACK) {
         // uneven spread: bitonic leaves + merge path on the same keys
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
@@ -211,6 +226,10 @@ __device__ bool block_slot_sort(Load load, Store store, uint32_t c, unsigned cha
         }
         block_merge_sort<K, THREADS, IPT>(s, c);
         for (uint32_t i = tid; i < c; i += THREADS) store(i, s[pidx(i)]);
+        refill();  // (after the merge, which needs the registers)
+    } else {
+        if (tid == 0) uneven();
+        refill();
     }
     __syncthreads();
     return even;

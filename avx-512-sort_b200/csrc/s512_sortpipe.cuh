@@ -126,6 +126,7 @@ struct LevelCtl {
     uint64_t level_keys;      // keys partitioned this level
     uint32_t learned_used;    // segments routed by their learned model
     uint32_t plain_used;      // segments routed by the splitter tree
+    uint32_t n_uneven[NCLASS];  // leaves handed from the slot sort to the block sort
 };
 
 // ===========================================================================
@@ -900,20 +901,54 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
 }
 
 // One block per bucket of at most THREADS*EPT keys: distribution counting
-// into value slots, or bitonic leaves + merge path when the slots come out
-// uneven (s512_slotsort.cuh).
+// into value slots (s512_slotsort.cuh).  The next bucket's keys are loaded
+// into registers while the current one is ranked and written.  A bucket whose
+// slots come out uneven is appended to `uneven` (count in *n_uneven) for
+// leaf_merge_kernel.
 template <typename K, typename OutCodec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems,
-                                                             OutCodec out) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+    leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems, OutCodec out, LeafItem<K>* uneven,
+                      uint32_t* n_uneven) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ SlotRed<K> red;
+    uint32_t it = blockIdx.x;
+    if (it >= nitems) return;
+    LeafItem<K> cur = items[it];
+    K key[EPT];
+    auto load = [&](const LeafItem<K>& item) {
+#pragma unroll
+        for (int r = 0; r < EPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + threadIdx.x;
+            if (i < item.count) key[r] = __ldg(item.src + i);
+        }
+    };
+    load(cur);
+    for (; it < nitems; it += gridDim.x) {
+        const uint32_t nx = it + gridDim.x;
+        LeafItem<K> next;
+        next.count = 0;
+        if (nx < nitems) next = items[nx];
+        const size_t dst = cur.dst;
+        block_slot_sort<K, THREADS, EPT, false>(
+            key, cur.count, [&](uint32_t i, K x) { out.store(dst + i, x); }, [&]() { load(next); },
+            [&]() { uneven[atomicAdd(n_uneven, 1u)] = cur; }, smem_raw, red);
+        cur = next;
+    }
+}
+
+// The buckets leaf_block_kernel found uneven: bitonic leaves + merge path.
+template <typename K, typename OutCodec, int THREADS, int EPT>
+__global__ void __launch_bounds__(THREADS) leaf_merge_kernel(const LeafItem<K>* __restrict__ items,
+                                                             const uint32_t* n_items, OutCodec out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K* s = reinterpret_cast<K*>(smem_raw);
+    const uint32_t nitems = *n_items;
     for (uint32_t it = blockIdx.x; it < nitems; it += gridDim.x) {
         const LeafItem<K> item = items[it];
-        const K* __restrict__ src = item.src;
-        const size_t dst = item.dst;
-        block_slot_sort<K, THREADS, EPT>([&](uint32_t i) { return src[i]; },
-                                         [&](uint32_t i, K x) { out.store(dst + i, x); }, item.count, smem_raw,
-                                         red);
+        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) s[pidx(i)] = item.src[i];
+        block_merge_sort<K, THREADS, EPT>(s, item.count);
+        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) out.store(item.dst + i, s[pidx(i)]);
+        __syncthreads();
     }
 }
 
@@ -949,11 +984,18 @@ __global__ void __launch_bounds__(32) small_warp_sort_kernel(InCodec in, OutCode
 }
 
 template <typename InCodec, typename OutCodec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) small_block_sort_kernel(InCodec in, OutCodec out, uint32_t n) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) small_block_sort_kernel(InCodec in, OutCodec out,
+                                                                                   uint32_t n) {
     using K = typename InCodec::Key;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ SlotRed<K> red;
-    block_slot_sort<K, THREADS, EPT>([&](uint32_t i) { return in.load(i); },
-                                     [&](uint32_t i, K x) { out.store(i, x); }, n, smem_raw, red);
+    K key[EPT];
+#pragma unroll
+    for (int r = 0; r < EPT; ++r) {
+        const uint32_t i = (uint32_t)r * THREADS + threadIdx.x;
+        if (i < n) key[r] = in.load(i);
+    }
+    block_slot_sort<K, THREADS, EPT, true>(
+        key, n, [&](uint32_t i, K x) { out.store(i, x); }, [] {}, [] {}, smem_raw, red);
 }
 }  // namespace s512

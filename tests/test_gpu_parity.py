@@ -285,6 +285,41 @@ def test_large_double_distributions(dist, s512, cuda):
     assert torch.equal(t, torch.sort(t0).values)
 
 
+@pytest.mark.parametrize("copies", [8, 40, 300])
+def test_leaves_with_repeated_values(copies, s512, cuda):
+    # every value repeated ~`copies` times, too rarely to become an equality
+    # bucket: a leaf's value slots hold runs of equal keys, which sends the
+    # leaf (copies >= 8 or so) from the slot sort to the block sort
+    import torch
+    n = 1 << 22
+    g = torch.Generator(device=cuda).manual_seed(copies)
+    distinct = n // copies
+    vals = torch.randint(-(1 << 30), 1 << 30, (distinct,), generator=g, device=cuda, dtype=torch.int64)
+    pick = torch.randint(0, distinct, (n,), generator=g, device=cuda)
+    t0 = vals[pick].to(torch.int32)
+    t = t0.clone()
+    s512.sort(t)
+    assert torch.equal(t, torch.sort(t0).values)
+    d0 = vals[pick].to(torch.float64) * 1e-3
+    d = d0.clone()
+    s512.sort(d)
+    assert torch.equal(d, torch.sort(d0).values)
+
+
+def test_leaves_mixed_even_and_uneven(s512, cuda):
+    # half the keys uniform (slot sort), half a few thousand repeated values
+    # in another range (block sort), in one array
+    import torch
+    n = (1 << 23) + 777
+    g = torch.Generator(device=cuda).manual_seed(5)
+    u = torch.rand(n, generator=g, device=cuda, dtype=torch.float64)
+    coarse = torch.floor(u * 4096.0) / 4096.0 + 2.0
+    t0 = torch.where(torch.arange(n, device=cuda) % 2 == 0, u, coarse)
+    t = t0.clone()
+    s512.sort(t)
+    assert torch.equal(t, torch.sort(t0).values)
+
+
 @pytest.mark.parametrize("keys", ["uniform", "zipf"])
 def test_large_kv(keys, s512, cuda):
     import torch
