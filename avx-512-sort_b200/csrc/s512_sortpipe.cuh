@@ -32,6 +32,7 @@ namespace s512 {
 constexpr int NB = 256;            // buckets per segment per pass (max)
 constexpr int SAMPLE_N = 16384;    // keys sampled per segment
 constexpr int COPY_CHUNK = 16384;  // equality buckets are copied in chunks of this size
+constexpr int SPLIT_SLOTS = 4096;  // value slots of the splitter lookup table
 constexpr unsigned long long ST_INC = 1ull << 63;  // status: inclusive prefix
 constexpr unsigned long long ST_AGG = 1ull << 62;  // status: tile aggregate only
 constexpr unsigned long long ST_VAL = (1ull << 62) - 1;
@@ -61,6 +62,14 @@ struct SplitSet {
     uint32_t has_eq;
     uint32_t nuniq;
     uint32_t pad_;
+    // Lookup table over the sample's value range: keys are clamped to
+    // [slot_map.lo, slot_hi] and mapped to SPLIT_SLOTS slots by slot_map;
+    // slot_tab[s] is the number of unique splitters whose slot is below s, so
+    // the splitters that a key of slot s still has to be compared with are
+    // uniq[slot_tab[s] .. slot_tab[s+1]).
+    SlotMap<K> slot_map;
+    K slot_hi;
+    alignas(16) uint8_t slot_tab[SPLIT_SLOTS + 4];
 };
 
 // A bucket that a leaf kernel sorts (or copies) into its final place.
@@ -222,6 +231,25 @@ __global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ sam
         eqf[t] = 0;
     }
     __syncthreads();
+    // splitter lookup table over [sample min, sample max]
+    {
+        __shared__ uint32_t sk[NB];
+        const SlotMap<K> f = make_slot_map<K>(smp[0], smp[m - 1], (uint32_t)SPLIT_SLOTS);
+        sk[t] = t < (int)K_u ? f(uniq[t]) : 0xFFFFFFFFu;
+        if (t == 0) {
+            out->slot_map = f;
+            out->slot_hi = smp[m - 1];
+        }
+        __syncthreads();
+        for (uint32_t s = t; s < (uint32_t)SPLIT_SLOTS + 4; s += NB) {
+            uint32_t lo = 0, hi = K_u;  // splitters with slot < s
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (sk[mid] < s) lo = mid + 1; else hi = mid;
+            }
+            out->slot_tab[s] = (uint8_t)lo;
+        }
+    }
     // bucket ids: range_j, then eq_j if splitter j has one; the last range bucket is K_u
     const uint32_t my_eq = (t < (int)K_u) ? eqf[t] : 0u;
     const uint32_t eq_before = block_exclusive_scan_first<NB, uint32_t>(my_eq, wtot, &total_eq);
@@ -305,6 +333,28 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
     return range_b[j];
 }
 
+// The same bucket through the splitter lookup table: the key's slot gives the
+// unique splitters below it up to the few that share its slot, which a binary
+// search over uniq[] settles (slot_tab is monotone, so tab[s] <= tab[s+1]).
+template <typename K>
+__device__ __forceinline__ uint32_t find_bucket_tab(const uint8_t* __restrict__ tab, const SlotMap<K>& f, K fhi,
+                                                    K x, bool has_eq, const K* __restrict__ uniq,
+                                                    const uint8_t* __restrict__ range_b,
+                                                    const uint8_t* __restrict__ eq_b,
+                                                    const uint32_t* __restrict__ eq_mask) {
+    const K xc = kmin(kmax(x, f.lo), fhi);
+    const uint32_t s = f(xc);
+    uint32_t lo = tab[s], hi = tab[s + 1];
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (uniq[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    const uint32_t j = lo;
+    if (!has_eq) return j;
+    if (j < 255 && ((eq_mask[j >> 5] >> (j & 31)) & 1u) && uniq[j] == x) return eq_b[j];
+    return range_b[j];
+}
+
 }  // namespace s512
 
 #include "s512_learned.cuh"
@@ -370,6 +420,9 @@ struct PartSmem {
     uint32_t eq_mask[NB / 32];
     uint64_t mbar[2];
     uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos, use_learned;
+    SlotMap<K> fmap;
+    K fhi;
+    alignas(16) uint8_t tab[SPLIT_SLOTS + 4];
     LearnedSet<K> L;
 };
 
@@ -486,9 +539,16 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
                     sm.eq_b[i] = ss.eq_b[i];
                 }
                 if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
+                {
+                    const uint32_t* src = reinterpret_cast<const uint32_t*>(ss.slot_tab);
+                    uint32_t* dst = reinterpret_cast<uint32_t*>(sm.tab);
+                    for (int i = tid; i < (SPLIT_SLOTS + 4) / 4; i += THREADS) dst[i] = src[i];
+                }
                 if (tid == 0) {
                     sm.has_eq = ss.has_eq;
                     sm.nbk = ss.nbuckets;
+                    sm.fmap = ss.slot_map;
+                    sm.fhi = ss.slot_hi;
                 }
             }
             if (tid == 0) sm.use_learned = use_learned ? 1u : 0u;
@@ -529,7 +589,8 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             // lanes past the end of the tile carry the out-of-range bucket NB
             if (idx >= cnt) bks[r] = (uint32_t)NB;
             else if (learned) bks[r] = learned_bucket<K>(sm.L, key[r]);
-            else bks[r] = find_bucket<K>(sm.tree, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b, sm.eq_mask);
+            else bks[r] = find_bucket_tab<K>(sm.tab, sm.fmap, sm.fhi, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b,
+                                             sm.eq_mask);
         }
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
