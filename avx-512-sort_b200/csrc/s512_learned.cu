@@ -92,7 +92,9 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
     const LearnedSet<K>* lp = ls;
     S512_CUDA_TRY(cudaMemcpyAsync(&h.loss_init, &lp->loss_init, 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaMemcpyAsync(&h.max_over_mean, &lp->max_over_mean, sizeof(float), cudaMemcpyDeviceToHost, st));
-    S512_CUDA_TRY(cudaMemcpyAsync(&h.nbuckets, &lp->nbuckets, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaMemcpyAsync(&h.nbuckets, &lp->nbuckets, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaMemcpyAsync(&h.nmodel, &lp->nmodel, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaMemcpyAsync(&h.ok, &lp->ok, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaStreamSynchronize(st));
     guard.finish();
     out->loss_init = h.loss_init;

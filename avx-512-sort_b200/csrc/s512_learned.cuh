@@ -50,19 +50,22 @@ struct LeafParam {
 
 template <typename K>
 struct LearnedSet {
+    // the model: everything inference reads, first, so that the partition
+    // pass can copy just this prefix (up to region_off) into shared memory
     K kmin;
     float inv_range;
+    uint32_t nmodel;     // model buckets
     float rc[LR_ROOT];   // root: value at the start of each piece (normalised)
     float rw[LR_ROOT];   // root: slope of each piece (normalised, >= 0)
     LeafParam<K> leaf[LR_LEAVES];
     K heavy[NB];         // per model bucket: its heavy key (if heavy_flag)
     uint8_t heavy_flag[NB];
     uint8_t base_id[NB]; // first bucket id of each model bucket
+    // bucket layout and diagnostics
     uint64_t region_off[NB];
     uint64_t region_cap[NB];
     uint32_t bucket_eq[NB / 32];
     uint32_t nbuckets;
-    uint32_t nmodel;     // model buckets
     uint32_t ok;         // 1: accepted (imbalance within bound)
     uint32_t pad_;
     float loss_init, loss_root, loss_final;

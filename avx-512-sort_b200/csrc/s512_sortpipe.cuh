@@ -25,6 +25,8 @@
 //     next partition level.
 #pragma once
 
+#include <cstddef>
+
 #include "s512_slotsort.cuh"
 
 namespace s512 {
@@ -379,7 +381,7 @@ namespace s512 {
 
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
 constexpr int CLAIM_GROUP = 4; // consecutive tiles a block claims at once (one table load per group)
-constexpr int LOOKBACK_W = 8;  // predecessor statuses read per look-back step
+constexpr int LOOKBACK_W = 2;  // predecessor statuses read per look-back step
 
 template <typename K>
 struct PartArgs {
@@ -400,13 +402,27 @@ struct PartArgs {
                                   // never-written status slot (0xFFFFFFFF: off)
 };
 
+// The routing tables of a plain split set, as the partition pass keeps them.
+template <typename K>
+struct PlainTables {
+    K uniq[NB];
+    uint8_t range_b[NB];
+    uint8_t eq_b[NB];
+    uint32_t eq_mask[NB / 32];
+    SlotMap<K> fmap;
+    K fhi;
+    alignas(16) uint8_t tab[SPLIT_SLOTS + 4];
+};
+
+// Bytes of a LearnedSet that inference reads (its leading fields).
+template <typename K>
+constexpr size_t learned_model_bytes() { return offsetof(LearnedSet<K>, region_off); }
+
 template <typename K, int THREADS, int IPT>
 struct PartSmem {
     static constexpr int TILE = THREADS * IPT;
     alignas(128) unsigned char buf[2][TILE * sizeof(K)];
     uint8_t bkt[TILE];
-    K tree[NB];
-    K uniq[NB];
     uint64_t region_off[NB];
     uint64_t region_cap[NB];
     uint64_t gdelta[NB];
@@ -414,20 +430,21 @@ struct PartSmem {
     uint32_t loc[NB];
     uint32_t seg_tile_start[SEG_SMEM];
     uint32_t wtot[8];
-    uint8_t range_b[NB];
-    uint8_t eq_b[NB];
     uint8_t ovf[NB];
-    uint32_t eq_mask[NB / 32];
     uint64_t mbar[2];
     uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos, use_learned;
-    SlotMap<K> fmap;
-    K fhi;
-    alignas(16) uint8_t tab[SPLIT_SLOTS + 4];
-    LearnedSet<K> L;
+    SegDesc sd;                   // segment of the tile being processed
+    SegDesc iss_sd;               // thread 0: segment of the last tile it fetched
+    uint32_t iss_seg;
+    // a segment routes by its split set or by its learned model, never both
+    union {
+        PlainTables<K> P;
+        alignas(16) unsigned char model[learned_model_bytes<K>()];
+    } T;
 };
 
 template <typename K, typename InCodec, int THREADS, int IPT>
-__global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, InCodec in) {
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(PartArgs<K> a, InCodec in) {
     extern __shared__ __align__(128) unsigned char smem_part[];
     using SM = PartSmem<K, THREADS, IPT>;
     SM& sm = *reinterpret_cast<SM*>(smem_part);
@@ -444,6 +461,7 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
         mbar_init(&sm.mbar[1], 1);
         fence_mbar_init();
         sm.abort = 0;
+        sm.iss_seg = 0xFFFFFFFFu;
     }
     for (int b = tid; b < NB; b += THREADS) sm.hist[b] = 0;
     if (small_tab)
@@ -463,7 +481,11 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
     // thread 0: start the bulk copy of tile t into buffer b
     auto issue = [&](uint32_t t, int b) {
         const uint32_t seg = seg_of(t);
-        const SegDesc sd = a.segs[seg];
+        if (seg != sm.iss_seg) {  // (tiles come in runs of one segment)
+            sm.iss_sd = a.segs[seg];
+            sm.iss_seg = seg;
+        }
+        const SegDesc sd = sm.iss_sd;
         const uint32_t ti = t - sd.tile_start;
         const uint64_t first = sd.in_off + (uint64_t)ti * TILE;
         const uint64_t rem = sd.count - (uint64_t)ti * TILE;
@@ -514,15 +536,17 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             claim_after = claim();  // consumed at the end of the iteration
             my_pos = atomicAdd(&a.chain[seg], 1u);
         }
-        const SegDesc sd = a.segs[seg];
         const bool new_seg = seg != cached_seg;
         if (new_seg) {
+            // the segment's descriptor and tables, read once per run of its tiles
+            if (tid < (int)(sizeof(SegDesc) / 4))
+                reinterpret_cast<uint32_t*>(&sm.sd)[tid] = reinterpret_cast<const uint32_t*>(&a.segs[seg])[tid];
             const bool use_learned = a.learned && a.learned[seg].ok;
             if (use_learned) {
                 const LearnedSet<K>& ls = a.learned[seg];
                 const uint32_t* src = reinterpret_cast<const uint32_t*>(&ls);
-                uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.L);
-                for (uint32_t i = tid; i < sizeof(LearnedSet<K>) / 4; i += THREADS) dst[i] = src[i];
+                uint32_t* dst = reinterpret_cast<uint32_t*>(sm.T.model);
+                for (uint32_t i = tid; i < learned_model_bytes<K>() / 4; i += THREADS) dst[i] = src[i];
                 for (int i = tid; i < NB; i += THREADS) {
                     sm.region_off[i] = ls.region_off[i];
                     sm.region_cap[i] = ls.region_cap[i];
@@ -531,34 +555,28 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             } else {
                 const SplitSet<K>& ss = a.splits[seg];
                 for (int i = tid; i < NB; i += THREADS) {
-                    sm.tree[i] = ss.tree[i];
-                    sm.uniq[i] = ss.uniq[i];
+                    sm.T.P.uniq[i] = ss.uniq[i];
                     sm.region_off[i] = ss.region_off[i];
                     sm.region_cap[i] = ss.region_cap[i];
-                    sm.range_b[i] = ss.range_b[i];
-                    sm.eq_b[i] = ss.eq_b[i];
+                    sm.T.P.range_b[i] = ss.range_b[i];
+                    sm.T.P.eq_b[i] = ss.eq_b[i];
                 }
-                if (tid < NB / 32) sm.eq_mask[tid] = ss.eq_mask[tid];
+                if (tid < NB / 32) sm.T.P.eq_mask[tid] = ss.eq_mask[tid];
                 {
                     const uint32_t* src = reinterpret_cast<const uint32_t*>(ss.slot_tab);
-                    uint32_t* dst = reinterpret_cast<uint32_t*>(sm.tab);
+                    uint32_t* dst = reinterpret_cast<uint32_t*>(sm.T.P.tab);
                     for (int i = tid; i < (SPLIT_SLOTS + 4) / 4; i += THREADS) dst[i] = src[i];
                 }
                 if (tid == 0) {
                     sm.has_eq = ss.has_eq;
                     sm.nbk = ss.nbuckets;
-                    sm.fmap = ss.slot_map;
-                    sm.fhi = ss.slot_hi;
+                    sm.T.P.fmap = ss.slot_map;
+                    sm.T.P.fhi = ss.slot_hi;
                 }
             }
             if (tid == 0) sm.use_learned = use_learned ? 1u : 0u;
             cached_seg = seg;
         }
-        const uint32_t ti = t - sd.tile_start;
-        const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
-        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
-        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
-        const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
         bool data_ok = true;
         if (a.tma) {
             // every thread waits on the barrier itself: the bulk copy's data is
@@ -567,7 +585,13 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             phase[b] ^= 1u;
             if (!data_ok) raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
         }
-        if (new_seg) __syncthreads();  // the segment's tables in shared memory
+        if (new_seg) __syncthreads();  // the segment's descriptor and tables in shared memory
+        const SegDesc sd = sm.sd;
+        const uint32_t ti = t - sd.tile_start;
+        const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
+        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
+        const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
+        const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
         const bool has_eq = sm.has_eq != 0;
         const bool learned = sm.use_learned != 0;
 
@@ -588,9 +612,12 @@ __global__ void __launch_bounds__(THREADS, 2) partition_kernel(PartArgs<K> a, In
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
             // lanes past the end of the tile carry the out-of-range bucket NB
             if (idx >= cnt) bks[r] = (uint32_t)NB;
-            else if (learned) bks[r] = learned_bucket<K>(sm.L, key[r]);
-            else bks[r] = find_bucket_tab<K>(sm.tab, sm.fmap, sm.fhi, key[r], has_eq, sm.uniq, sm.range_b, sm.eq_b,
-                                             sm.eq_mask);
+            else if (learned)
+                // (only the model prefix of the LearnedSet is in shared memory)
+                bks[r] = learned_bucket<K>(*reinterpret_cast<const LearnedSet<K>*>(sm.T.model), key[r]);
+            else
+                bks[r] = find_bucket_tab<K>(sm.T.P.tab, sm.T.P.fmap, sm.T.P.fhi, key[r], has_eq, sm.T.P.uniq,
+                                            sm.T.P.range_b, sm.T.P.eq_b, sm.T.P.eq_mask);
         }
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
