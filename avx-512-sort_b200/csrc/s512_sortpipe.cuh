@@ -347,9 +347,13 @@ __device__ __forceinline__ uint32_t find_bucket_tab(const uint8_t* __restrict__ 
     const K xc = kmin(kmax(x, f.lo), fhi);
     const uint32_t s = f(xc);
     uint32_t lo = tab[s], hi = tab[s + 1];
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (uniq[mid] < x) lo = mid + 1; else hi = mid;
+    if (hi - lo == 1) {  // the common case: one splitter shares the key's slot
+        lo += uniq[lo] < x ? 1u : 0u;
+    } else {
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (uniq[mid] < x) lo = mid + 1; else hi = mid;
+        }
     }
     const uint32_t j = lo;
     if (!has_eq) return j;
@@ -382,6 +386,7 @@ namespace s512 {
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
 constexpr int CLAIM_GROUP = 4; // consecutive tiles a block claims at once (one table load per group)
 constexpr int LOOKBACK_W = 2;  // predecessor statuses read per look-back step
+constexpr uint64_t GDELTA_DROP = ~0ull;  // write offset of a bucket that overflowed its region
 
 template <typename K>
 struct PartArgs {
@@ -430,7 +435,6 @@ struct PartSmem {
     uint32_t loc[NB];
     uint32_t seg_tile_start[SEG_SMEM];
     uint32_t wtot[8];
-    uint8_t ovf[NB];
     uint64_t mbar[2];
     uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos, use_learned;
     SegDesc sd;                   // segment of the tile being processed
@@ -736,16 +740,20 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
             const uint64_t end = prefix + h;
             const bool ovf = !ok || end > sm.region_cap[tid];
             if (ovf && h) raise_error(&a.ctl->err, ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
-            sm.ovf[tid] = ovf ? 1 : 0;
-            sm.gdelta[tid] = sd.out_base + sm.region_off[tid] + prefix - (uint64_t)sm.loc[tid];
+            sm.gdelta[tid] = ovf ? GDELTA_DROP : sd.out_base + sm.region_off[tid] + prefix - (uint64_t)sm.loc[tid];
             if (pos == sd.ntiles - 1) a.bucket_counts[(size_t)seg * NB + tid] = end;
         }
         __syncthreads();
 
-        // coalesced write-out
-        for (uint32_t i = tid; i < cnt; i += THREADS) {
-            const uint32_t bk = sm.bkt[i];
-            if (!sm.ovf[bk]) a.out[sm.gdelta[bk] + i] = stage[i];
+        // coalesced write-out (an overflowed bucket's keys are dropped: the
+        // level is redone)
+#pragma unroll
+        for (int r = 0; r < IPT; ++r) {
+            const uint32_t i = (uint32_t)(r * THREADS + tid);
+            if (i < cnt) {
+                const uint64_t g = sm.gdelta[sm.bkt[i]];
+                if (g != GDELTA_DROP) a.out[g + i] = stage[i];
+            }
         }
         if (tid < NB) sm.hist[tid] = 0;
         if (tid == 0) {
