@@ -162,7 +162,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     S512_LAUNCH_CHECK();
     {
         auto fn = sample_sort_kernel<K>;
-        const size_t smem = (size_t)padded_len(SAMPLE_N) * KB;
+        const size_t smem = SlotSmem<K, 1024, SAMPLE_N / 1024>::bytes;
         S512_CUDA_TRY(C.prepare((const void*)fn, smem));
         fn<<<nsegs, 1024, smem, st>>>(samples, L.segs, nsegs, KB);
         S512_LAUNCH_CHECK();

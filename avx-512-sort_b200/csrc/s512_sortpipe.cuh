@@ -162,12 +162,20 @@ template <typename K>
 __global__ void __launch_bounds__(1024) sample_sort_kernel(K* __restrict__ samples, const SegDesc* __restrict__ segs,
                                                            uint32_t nsegs, int key_bytes) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* s = reinterpret_cast<K*>(smem_raw);
+    __shared__ SlotRed<K> red;
+    constexpr int IPT = SAMPLE_N / 1024;
     const uint32_t m = sample_size(target_buckets(key_bytes, segs[blockIdx.x].count));
     K* p = samples + (size_t)blockIdx.x * SAMPLE_N;
-    for (uint32_t i = threadIdx.x; i < m; i += 1024) s[pidx(i)] = p[i];
-    block_merge_sort<K, 1024, SAMPLE_N / 1024>(s, m);
-    for (uint32_t i = threadIdx.x; i < m; i += 1024) p[i] = s[pidx(i)];
+    K key[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        const uint32_t i = (uint32_t)r * 1024 + threadIdx.x;
+        if (i < m) key[r] = p[i];
+    }
+    // samples are spread like the segment's keys: distribution counting,
+    // with the block sort for skewed samples (s512_slotsort.cuh)
+    block_slot_sort<K, 1024, IPT, true>(
+        key, m, [&](uint32_t i, K x) { p[i] = x; }, [] {}, [] {}, smem_raw, red);
 }
 
 // 3. Splitters and bucket regions: one block of 256 threads per segment.
@@ -384,7 +392,11 @@ namespace s512 {
 // read with plain loads instead (a.tma == 0).
 
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
-constexpr int CLAIM_GROUP = 4; // consecutive tiles a block claims at once (one table load per group)
+// Consecutive tiles a block claims at once: one segment's tables are loaded
+// once per group, so levels with many segments take longer runs; a single
+// segment takes short ones (a finer split of the last tiles among blocks).
+constexpr uint32_t CLAIM_GROUP_ONE_SEG = 4;
+constexpr uint32_t CLAIM_GROUP_MANY_SEGS = 16;
 constexpr int LOOKBACK_W = 2;  // predecessor statuses read per look-back step
 constexpr uint64_t GDELTA_DROP = ~0ull;  // write offset of a bucket that overflowed its region
 
@@ -506,13 +518,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
     };
 
     uint32_t claim_after = 0;  // thread 0: the tile claimed for two iterations ahead
-    // thread 0 claims CLAIM_GROUP consecutive tiles at a time, so that a block
+    const uint32_t claim_group = a.nsegs > 1 ? CLAIM_GROUP_MANY_SEGS : CLAIM_GROUP_ONE_SEG;
+    // thread 0 claims claim_group consecutive tiles at a time, so that a block
     // works through a run of one segment before it loads another's tables
     uint32_t grp_next = 0, grp_end = 0;
     auto claim = [&]() -> uint32_t {
         if (grp_next == grp_end) {
-            grp_next = atomicAdd(&a.ctl->tile_counter, (uint32_t)CLAIM_GROUP);
-            grp_end = grp_next + CLAIM_GROUP;
+            grp_next = atomicAdd(&a.ctl->tile_counter, claim_group);
+            grp_end = grp_next + claim_group;
         }
         return grp_next++;
     };
