@@ -24,6 +24,13 @@ import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+# DRAM bytes per key of one partition launch (read + write, ncu
+# dram__bytes_read.sum + dram__bytes_write.sum, mean of the two levels of a
+# 2^26-key double sort: 1058.9 MB and 1067.7 MB for 67,108,864 keys).  The
+# algorithmic figure is 16 B/key; the capture sits just below it because some
+# written lines are still in L2 when the kernel ends.  Traffic grows with the
+# keys, so the bench scales it to its own launch size.
+PART_DRAM_BYTES_PER_KEY = 15.84
 PKG = os.path.join(ROOT, "avx-512-sort_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
@@ -271,7 +278,10 @@ def run_ours(args, world, rank, local):
     roofline = {"bound": "hbm", "kernel": "partition_kernel" if dominant == "partition" else "leaf sorts",
                 "achieved": round(ach, 1) if ach else None, "peak": peak, "unit": "GB/s",
                 "frac": round(ach / peak, 4) if ach else None, "peak_source": peak_kind,
-                "traffic": None,
+                "traffic": (round(PART_DRAM_BYTES_PER_KEY * n) if dominant == "partition" else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per partition launch on a "
+                                  "2^26-key double sort (both levels), %.2f B/key, scaled to n keys per launch"
+                                  % PART_DRAM_BYTES_PER_KEY,
                 "partition_kernel": {"achieved": round(part_gbs, 1) if part_gbs else None,
                                      "frac": round(part_gbs / peak, 4) if part_gbs else None,
                                      "ms_per_step": round(tot_part_ms / args.steps, 3),
@@ -466,12 +476,18 @@ def extra_learned(dev, stream):
         row = {"n": n}
         for mode, flag in (("plain", s512.SPLIT_PLAIN), ("learned", s512.SPLIT_LEARNED)):
             x = x0.clone()
-            s512.sort(x, flags=flag | s512.ASYNC, stream=stream)  # warm
-            x.copy_(x0)
-            ms = _timed(lambda: s512.sort(x, flags=flag | s512.ASYNC, stream=stream), stream)
+            for _ in range(2):  # warm: scratch sized and kernels loaded for this mode
+                x.copy_(x0)
+                s512.sort(x, flags=flag | s512.ASYNC, stream=stream)
+            times = []
+            for _ in range(3):
+                x.copy_(x0)
+                times.append(_timed(lambda: s512.sort(x, flags=flag | s512.ASYNC, stream=stream), stream))
+            ms = sorted(times)[1]
             st = s512.stats()
             row[mode] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
                          "partition_ms": round(sum(st["partition_ms"]), 3),
+                         "sample_and_fit_ms": round(sum(st["sample_ms"]), 3),
                          "levels": st["levels"], "model_levels": st["learned_levels"],
                          "models_rejected": st["learned_rejected"], "fallbacks": st["fallbacks"],
                          "max_bucket_over_mean": [round(v, 2) for v in st["max_bucket_over_mean"]],
