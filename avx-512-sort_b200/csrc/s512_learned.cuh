@@ -35,6 +35,9 @@
 
 namespace s512 {
 
+// Segments below this many keys are not fitted: a partition pass over them
+// is short next to the fit (the levels with thousands of small segments).
+constexpr uint64_t LR_MIN_KEYS = 1ull << 19;
 constexpr int LR_ROOT = 64;
 constexpr int LR_LEAVES = 256;
 constexpr int LR_THREADS = 512;
@@ -215,10 +218,14 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
     __shared__ LearnedSet<K> L;  // built here, copied out at the end
 
     const SegDesc sd = segs[sgi];
+    const int tid = threadIdx.x;
+    if (sd.count < LR_MIN_KEYS) {  // too small to repay a fit: the split set routes it
+        if (tid == 0) out[sgi].ok = 0;
+        return;
+    }
     const int nb = target_buckets(key_bytes, sd.count);
     const uint32_t m = sample_size(nb);
     const K* smp = samples + (size_t)sgi * SAMPLE_N;
-    const int tid = threadIdx.x;
 
     // coordinate
     const K kmin = smp[0], kmax = smp[m - 1];
