@@ -88,9 +88,9 @@ static int launch_small(DevCtx& C, Codec io, const SegItem* wi, const SegItem* b
                         bool prepare_only) {
     using K = typename Codec::Key;
     auto fn = segsort_small_kernel<Codec, T, E>;
-    const uint32_t keys = padded_len(T * E) > (uint32_t)(T / 32) * WARP_REGION ? padded_len(T * E)
-                                                                                : (uint32_t)(T / 32) * WARP_REGION;
-    const size_t smem = (size_t)keys * sizeof(K);
+    const size_t block_bytes = SlotSmem<K, T, E>::bytes;
+    const size_t warp_bytes = (size_t)(T / 32) * WARP_REGION * sizeof(K);
+    const size_t smem = block_bytes > warp_bytes ? block_bytes : warp_bytes;
     int grid = 0;
     S512_CUDA_TRY(launch_persistent(C, fn, T, smem, st, 0, &grid));
     if (prepare_only) return S512_OK;

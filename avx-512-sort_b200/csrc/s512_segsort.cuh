@@ -4,9 +4,10 @@
 // independent arrays (sort512perf.cpp:612-709 timeSmall).  Here a batch of
 // segments is classified once by length, then one persistent launch sorts
 // every segment of up to a block's capacity: blocks first take "block"
-// segments from an atomic queue (bitonic leaves + merge path, one block per
-// segment), then every warp takes "warp" segments of at most 256 keys (one
-// bitonic network per warp).  Longer segments run the partition levels.
+// segments from an atomic queue (one block per segment: the slot sort of
+// s512_slotsort.cuh, with the bitonic + merge-path block sort for segments
+// whose values are unevenly spread), then every warp takes "warp" segments of
+// at most 256 keys (one bitonic network per warp).  Longer segments run the partition levels.
 #pragma once
 
 #include "s512_blocksort.cuh"
@@ -77,13 +78,14 @@ __global__ void segsort_classify_kernel(const size_t* __restrict__ offsets, size
 // The persistent launch for warp and block segments.  io reads and writes the
 // caller's layout in place.
 template <typename Codec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS) segsort_small_kernel(Codec io, const SegItem* __restrict__ warp_items,
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) segsort_small_kernel(Codec io, const SegItem* __restrict__ warp_items,
                                                                 const SegItem* __restrict__ block_items,
                                                                 SegCtl* __restrict__ ctl) {
     using K = typename Codec::Key;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K* s = reinterpret_cast<K*>(smem_raw);
     __shared__ uint32_t s_item;
+    __shared__ SlotRed<K> red;
     const uint32_t nblock = ctl->n_block;
     const uint32_t nwarp = ctl->n_warp;
 
@@ -95,10 +97,14 @@ __global__ void __launch_bounds__(THREADS) segsort_small_kernel(Codec io, const 
         __syncthreads();
         if (it >= nblock) break;
         const SegItem item = block_items[it];
-        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) s[pidx(i)] = io.load(item.off + i);
-        block_merge_sort<K, THREADS, EPT>(s, item.count);
-        for (uint32_t i = threadIdx.x; i < item.count; i += THREADS) io.store(item.off + i, s[pidx(i)]);
-        __syncthreads();
+        K key[EPT];
+#pragma unroll
+        for (int r = 0; r < EPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + threadIdx.x;
+            if (i < item.count) key[r] = io.load(item.off + i);
+        }
+        block_slot_sort<K, THREADS, EPT, true>(
+            key, item.count, [&](uint32_t i, K x) { io.store(item.off + i, x); }, [] {}, [] {}, smem_raw, red);
     }
 
     // warp segments
