@@ -7,10 +7,15 @@
 
 namespace s512 {
 
-// Tile shapes of the partition kernel per key size.
+// Tile shapes of the partition kernel per key size: levels with many segments
+// (PartShape), and a level that is one whole array (PartShapeOne), where a
+// bigger tile halves the look-back walks of the single chain.
 template <typename K> struct PartShape;
 template <> struct PartShape<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
 template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT = 8; };
+template <typename K> struct PartShapeOne;
+template <> struct PartShapeOne<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
+template <> struct PartShapeOne<uint64_t> { static constexpr int THREADS = 1024, IPT = 8; };
 
 // ---------------------------------------------------------------------------
 // leaf launches per class
@@ -125,13 +130,11 @@ struct Level {
     bool aligned;               // every tile starts 16-byte aligned (bulk copies allowed)
 };
 
-template <typename K, typename InCodec, typename UserOut>
+template <typename K, typename InCodec, typename UserOut, typename Shape = PartShape<K>>
 static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, size_t n, cudaStream_t st,
                      LevelCtl* ctl, LevelCtl* next_ctl_dev, SegDesc* next_segs, uint32_t next_cap,
                      PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl, bool learned) {
     constexpr int KB = sizeof(K);
-    using Shape = PartShape<K>;
-    constexpr int TILE = Shape::THREADS * Shape::IPT;
     const uint32_t nsegs = L.nsegs;
     int rc;
 
@@ -317,13 +320,20 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
 // final_off set).  A single segment starting at element 0 is laid out here;
 // several segments are laid out by prepare_level_kernel.  Buckets that fit a
 // leaf are sorted straight into their final place in the caller's array.
+//
+// `whole` says that segs0 is one segment covering the caller's array from
+// element 0 with its tile fields set (sort_pipeline); any other list, even of
+// one segment, is laid out on the device (a lone segment of a batch starts
+// wherever the caller's segment starts, so its tiles need not be 16-byte
+// aligned for the bulk copy).
 template <typename K, typename UserIn, typename UserOut>
 static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint32_t nsegs0, uint64_t keys0,
-                      cudaStream_t st, PhaseTimer& tm, s512_stats& S, bool learned = false) {
+                      cudaStream_t st, PhaseTimer& tm, s512_stats& S, bool whole, bool learned = false) {
     constexpr int KB = sizeof(K);
     using Shape = PartShape<K>;
     constexpr int TILE = Shape::THREADS * Shape::IPT;
-    const bool single = nsegs0 == 1;
+    constexpr int TILE_ONE = PartShapeOne<K>::THREADS * PartShapeOne<K>::IPT;
+    const bool single = whole && nsegs0 == 1;
 
     // Level buffers T0 / T1 alternate as partition outputs.  A level's output
     // needs the sum over its segments of region_bound(count) rounded to 16
@@ -349,7 +359,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
     L0.out = T[0];
     if (single) {
         L0.tile_seg = nullptr;
-        L0.ntiles_host = (uint32_t)((keys0 + TILE - 1) / TILE);
+        L0.ntiles_host = (uint32_t)((keys0 + TILE_ONE - 1) / TILE_ONE);
         L0.ntiles_dev = nullptr;
         L0.ntiles_bound = L0.ntiles_host;
         L0.aligned = true;
@@ -369,8 +379,10 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         L0.ntiles_bound = bound;
         L0.aligned = false;  // segment starts are wherever the caller's segments start
     }
-    int rc = run_level<K, UserIn, UserOut>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1], segbuf[1], next_cap, tm,
-                                           S, host_ctl, learned);
+    int rc = single ? run_level<K, UserIn, UserOut, PartShapeOne<K>>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1],
+                                                                      segbuf[1], next_cap, tm, S, host_ctl, learned)
+                    : run_level<K, UserIn, UserOut>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1], segbuf[1],
+                                                    next_cap, tm, S, host_ctl, learned);
     if (rc) return rc;
     S.levels = 1;
 
@@ -428,7 +440,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
 // The whole pipeline for one array of n > leaf_max keys.
 template <typename K, typename UserIn, typename UserOut>
 static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned) {
-    constexpr int TILE = PartShape<K>::THREADS * PartShape<K>::IPT;
+    constexpr int TILE = PartShapeOne<K>::THREADS * PartShapeOne<K>::IPT;  // a single segment
     s512_stats& S = thread_stats();
     PhaseTimer tm(st, config().collect_stats != 0);
     const int tstart = tm.mark();
@@ -442,7 +454,7 @@ static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStre
     s0.tile_start = 0;
     s0.ntiles = (uint32_t)((n + TILE - 1) / TILE);
     S512_CUDA_TRY(cudaMemcpyAsync(seg0, &s0, sizeof(SegDesc), cudaMemcpyHostToDevice, st));
-    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S, learned);
+    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S, true, learned);
     if (rc) return rc;
     const int tend = tm.mark();
     if (tm.on()) S.total_ms = tm.ms(tstart, tend);

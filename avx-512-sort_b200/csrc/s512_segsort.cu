@@ -142,7 +142,7 @@ template <typename K, typename Codec>
 static int sort_big(DevCtx& C, Codec io, const SegLists& L, uint32_t n_big, uint64_t big_keys, cudaStream_t st,
                     PhaseTimer& tm, s512_stats& S) {
     if (n_big == 0) return S512_OK;
-    return run_levels<K, Codec, Codec>(C, io, io, L.big, n_big, big_keys, st, tm, S);
+    return run_levels<K, Codec, Codec>(C, io, io, L.big, n_big, big_keys, st, tm, S, false);
 }
 
 // The whole batch on the device: classify, persistent launch, long segments.

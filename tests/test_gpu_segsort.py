@@ -39,6 +39,21 @@ def test_segsort_edge_layouts(s512, cuda, oracle):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("lens", [[3, 100001, 5], [70001], [1, 0, 40000, 2]])
+def test_segsort_one_long_segment(lens, s512, cuda, oracle):
+    # exactly one segment above a block's capacity, at an odd offset or alone:
+    # it runs the partition levels as a batch of one
+    import workloads
+    off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    for dt in (np.int32, np.float64):
+        n = int(off[-1])
+        a = workloads.uniform_i32_np(n, 8) if dt == np.int32 else workloads.uniform01_np(n, 8)
+        b = a.copy()
+        s512.segsort(a, off)
+        oracle.segsort(b, off)
+        assert np.array_equal(a, b), (lens, dt)
+
+
 def test_segsort_device_and_kv(s512, cuda):
     import torch
     import workloads
