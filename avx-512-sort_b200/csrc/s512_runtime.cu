@@ -90,7 +90,11 @@ void DevCtx::release_all() {
 cudaError_t DevCtx::prepare(const void* fn, size_t smem) {
     auto it = smem_set.find(fn);
     if (it != smem_set.end() && it->second >= smem) return cudaSuccess;
-    if (smem > 48 * 1024) {
+    // the 48 KB default covers static + dynamic shared memory together
+    cudaFuncAttributes fa;
+    cudaError_t ea = cudaFuncGetAttributes(&fa, fn);
+    if (ea != cudaSuccess) return ea;
+    if (smem + fa.sharedSizeBytes > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         // prefer the largest shared-memory carveout so that several such

@@ -65,11 +65,12 @@ struct SlotRed {
 };
 
 // Shared memory of block_slot_sort for a block of THREADS x IPT keys: the
-// key buffer (padded for the fallback block sort) followed by the counters.
-template <typename K, int THREADS, int IPT>
+// key buffer (padded for the block sort when that runs inline, INLINE) and
+// the counters.
+template <typename K, int THREADS, int IPT, bool INLINE = true>
 struct SlotSmem {
     static constexpr uint32_t S = (uint32_t)THREADS * IPT;
-    static constexpr size_t keys_bytes = ((size_t)padded_len(S) * sizeof(K) + 15) & ~(size_t)15;
+    static constexpr size_t keys_bytes = ((size_t)(INLINE ? padded_len(S) : S) * sizeof(K) + 15) & ~(size_t)15;
     static constexpr size_t bytes = keys_bytes + (size_t)S * sizeof(uint32_t);
 };
 
@@ -93,7 +94,7 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
     constexpr int NW = THREADS / 32;
     static_assert(IPT % 4 == 0, "counters are read four at a time");
     K* s = reinterpret_cast<K*>(smem);
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SlotSmem<K, THREADS, IPT>::keys_bytes);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SlotSmem<K, THREADS, IPT, INLINE_FALLBACK>::keys_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
     // 1. bounds of the bucket; counters zeroed

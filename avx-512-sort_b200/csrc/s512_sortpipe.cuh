@@ -84,12 +84,16 @@ struct LeafItem {
 };
 
 // Leaf size classes.  Class 0 is one warp per bucket (a 256-key bitonic
-// leaf); the others are one block per bucket (bitonic leaves + merge path,
-// s512_blocksort.cuh).  The copy list holds equality buckets.
-constexpr int NCLASS = 6;
+// leaf); the others are one block per bucket (the slot sort of
+// s512_slotsort.cuh, with the bitonic + merge-path block sort for uneven
+// buckets).  A bucket's class is the smallest that holds it, so its keys fill
+// between 2/3 and all of the class's slots above 4096.  The copy list holds
+// equality buckets.
+constexpr int NCLASS = 7;
 constexpr int CLS_COPY = NCLASS;  // index of the copy list
 __host__ __device__ constexpr int class_cap(int c) {
-    return c == 0 ? 256 : (512 << c);  // 256, 1024, 2048, 4096, 8192, 16384
+    // 256 | 1024 2048 4096 6144 8192 16384
+    return c == 0 ? 256 : c == 4 ? 6144 : (c < 4 ? (512 << c) : (512 << (c - 1)));
 }
 __host__ __device__ constexpr uint32_t leaf_max(int /*key_bytes*/) { return 16384u; }
 __host__ __device__ inline int class_of(int /*key_bytes*/, uint32_t count) {
@@ -1009,13 +1013,17 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
     }
 }
 
+// Blocks per SM that the leaf kernel's register budget is sized for (the
+// 384-thread class fits three, with its keys' shared memory unpadded).
+__host__ __device__ constexpr int leaf_min_blocks(int threads) { return threads == 384 ? 3 : 1024 / threads; }
+
 // One block per bucket of at most THREADS*EPT keys: distribution counting
 // into value slots (s512_slotsort.cuh).  The next bucket's keys are loaded
 // into registers while the current one is ranked and written.  A bucket whose
 // slots come out uneven is appended to `uneven` (count in *n_uneven) for
 // leaf_merge_kernel.
 template <typename K, typename OutCodec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+__global__ void __launch_bounds__(THREADS, leaf_min_blocks(THREADS))
     leaf_block_kernel(const LeafItem<K>* __restrict__ items, uint32_t nitems, OutCodec out, LeafItem<K>* uneven,
                       uint32_t* n_uneven) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
