@@ -26,11 +26,11 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 # DRAM bytes per key of one partition launch (read + write, ncu
 # dram__bytes_read.sum + dram__bytes_write.sum, mean of the two levels of a
-# 2^26-key double sort: 1058.9 MB and 1067.7 MB for 67,108,864 keys).  The
+# 2^26-key double sort: 1042.3 MB and 1068.2 MB for 67,108,864 keys).  The
 # algorithmic figure is 16 B/key; the capture sits just below it because some
 # written lines are still in L2 when the kernel ends.  Traffic grows with the
 # keys, so the bench scales it to its own launch size.
-PART_DRAM_BYTES_PER_KEY = 15.84
+PART_DRAM_BYTES_PER_KEY = 15.72
 PKG = os.path.join(ROOT, "avx-512-sort_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
