@@ -309,9 +309,12 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         }
         (void)t3;
         // imbalance: largest bucket over the mean non-empty bucket of the level
-        if (host_ctl->nonempty && host_ctl->level_keys)
-            S.max_bucket_over_mean[level] =
-                (double)host_ctl->max_bucket / ((double)host_ctl->level_keys / (double)host_ctl->nonempty);
+        if (host_ctl->nonempty && host_ctl->level_keys) {
+            const double mean = (double)host_ctl->level_keys / (double)host_ctl->nonempty;
+            S.max_bucket_over_mean[level] = (double)host_ctl->max_bucket / mean;
+            const double var = host_ctl->bucket_sq / (double)host_ctl->nonempty - mean * mean;
+            S.bucket_cv[level] = var > 0.0 ? sqrt(var) / mean : 0.0;
+        }
     }
     (void)next_ctl_dev;
     return S512_OK;

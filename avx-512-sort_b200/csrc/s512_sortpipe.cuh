@@ -142,6 +142,7 @@ struct LevelCtl {
     uint32_t learned_used;    // segments routed by their learned model
     uint32_t plain_used;      // segments routed by the splitter tree
     uint32_t n_uneven[NCLASS];  // leaves handed from the slot sort to the block sort
+    double bucket_sq;         // sum of squared non-empty bucket sizes this level
 };
 
 // ===========================================================================
@@ -892,6 +893,7 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
     atomicMax(&a.ctl->max_bucket, (uint32_t)(c > 0xFFFFFFFFull ? 0xFFFFFFFFull : c));
     atomicAdd(&a.ctl->nonempty, 1u);
     atomicAdd((unsigned long long*)&a.ctl->level_keys, (unsigned long long)c);
+    atomicAdd(&a.ctl->bucket_sq, (double)c * (double)c);
     const K* src = a.level_out + sd.out_base + region_off[b];
     const uint64_t dst = sd.final_off + excl;
     const bool is_eq = (bucket_eq[b >> 5] >> (b & 31)) & 1u;

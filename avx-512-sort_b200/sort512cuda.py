@@ -75,6 +75,7 @@ class Stats(ctypes.Structure):
         ("max_bucket_over_mean", ctypes.c_double * MAX_LEVELS),
         ("kernel_launches", ctypes.c_uint32),
         ("key_bytes", ctypes.c_uint32),
+        ("bucket_cv", ctypes.c_double * MAX_LEVELS),
     ]
 
     def as_dict(self) -> dict:
@@ -93,6 +94,7 @@ class Stats(ctypes.Structure):
             "max_bucket_over_mean": list(self.max_bucket_over_mean[:lv]),
             "kernel_launches": int(self.kernel_launches),
             "key_bytes": int(self.key_bytes),
+            "bucket_cv": list(self.bucket_cv[:lv]),
         }
 
 

@@ -491,6 +491,7 @@ def extra_learned(dev, stream):
                          "levels": st["levels"], "model_levels": st["learned_levels"],
                          "models_rejected": st["learned_rejected"], "fallbacks": st["fallbacks"],
                          "max_bucket_over_mean": [round(v, 2) for v in st["max_bucket_over_mean"]],
+                         "bucket_cv": [round(v, 3) for v in st["bucket_cv"]],
                          "sorted": bool((x[1:] >= x[:-1]).all())}
             del x
         rows[name] = row

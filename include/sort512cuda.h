@@ -100,6 +100,7 @@ typedef struct s512_stats {
     double max_bucket_over_mean[S512_MAX_LEVELS]; /* bucket imbalance per level */
     uint32_t kernel_launches;               /* kernels launched by the call */
     uint32_t key_bytes;                     /* 4 or 8 */
+    double bucket_cv[S512_MAX_LEVELS];      /* std / mean of the non-empty bucket sizes, per level */
 } s512_stats;
 
 /* --- configuration, errors, resources ---------------------------------- */
