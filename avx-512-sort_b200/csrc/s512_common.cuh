@@ -131,6 +131,44 @@ struct CodecKV {
     }
 };
 
+// int64 keys: uint64 k = x ^ 2^63 (signed order).
+struct CodecI64 {
+    using Key = uint64_t;
+    static constexpr int NARR = 1;
+    static constexpr int ESZ = 8;
+    const unsigned long long* __restrict__ in;
+    unsigned long long* __restrict__ out;
+    __device__ __forceinline__ uint64_t load(size_t i) const { return __ldg(in + i) ^ 0x8000000000000000ull; }
+    __device__ __forceinline__ void store(size_t i, uint64_t k) const { out[i] = k ^ 0x8000000000000000ull; }
+    __host__ __device__ const void* arr(int) const { return in; }
+    __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
+        return reinterpret_cast<const unsigned long long*>(buf)[i] ^ 0x8000000000000000ull;
+    }
+};
+
+// int key + int value interleaved as pairs (int[2]: key first): one 64-bit
+// word per pair (little-endian: key in the low half), encoded like CodecKV.
+struct CodecKVPairs {
+    using Key = uint64_t;
+    static constexpr int NARR = 1;
+    static constexpr int ESZ = 8;
+    const unsigned long long* __restrict__ in;
+    unsigned long long* __restrict__ out;
+    static __device__ __forceinline__ uint64_t enc(unsigned long long w) {
+        return enc_kv((int)(uint32_t)w, (int)(uint32_t)(w >> 32));
+    }
+    __device__ __forceinline__ uint64_t load(size_t i) const { return enc(__ldg(in + i)); }
+    __device__ __forceinline__ void store(size_t i, uint64_t k) const {
+        const uint32_t key = (uint32_t)dec_i32((uint32_t)(k >> 32));
+        const uint32_t val = (uint32_t)dec_i32((uint32_t)k);
+        out[i] = ((unsigned long long)val << 32) | key;
+    }
+    __host__ __device__ const void* arr(int) const { return in; }
+    __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
+        return enc(reinterpret_cast<const unsigned long long*>(buf)[i]);
+    }
+};
+
 // Codec that reads the library's encoded scratch and writes the caller's layout.
 template <typename K, typename OutCodec>
 struct RawToUser {

@@ -1,0 +1,46 @@
+// s512_sort64.cu -- the sort for 64-bit words that the reference's interface
+// describes but does not implement: int64 keys, and int key/value pairs stored
+// interleaved as int[2] (the reference's README speaks of sorting "int[2]";
+// its kv interface, sort512kv.hpp:6133, takes two separate arrays).  Same
+// pipeline as s512_sort.cu, through the CodecI64 / CodecKVPairs codecs.
+#include "s512_pipeline.cuh"
+
+using namespace s512;
+
+namespace s512 {
+
+template <typename Codec, typename T>
+static int sort_words(T* data, size_t n, int flags, void* stream) {
+    if (n == 0) return S512_OK;
+    if (!data) return S512_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    int status = S512_OK;
+    DevCtx* C = current_ctx(&status);
+    if (!C) return status;
+    CallGuard guard(C, st);
+    const bool host = pointer_kind(data, flags) == 1;
+    unsigned long long* d = (unsigned long long*)data;
+    if (host) {
+        d = (unsigned long long*)C->get("stage0", n * 8);
+        if (!d) return S512_ERR_ALLOC;
+        S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * 8, cudaMemcpyHostToDevice, st));
+    }
+    int rc = sort_device<uint64_t>(*C, Codec{d, d}, Codec{d, d}, n, st, use_learned(flags));
+    if (rc) return rc;
+    if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * 8, cudaMemcpyDeviceToHost, st));
+    return finish_call(guard, st, flags, host);
+}
+
+}  // namespace s512
+
+extern "C" {
+
+int s512_sort_i64(long long* data, size_t n, int flags, void* stream) {
+    return sort_words<CodecI64>(data, n, flags, stream);
+}
+
+int s512_sort_kv_pairs_i32(int* pairs, size_t n, int flags, void* stream) {
+    return sort_words<CodecKVPairs>(reinterpret_cast<long long*>(pairs), n, flags, stream);
+}
+
+}  // extern "C"

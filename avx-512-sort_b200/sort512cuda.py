@@ -47,6 +47,7 @@ EXPORTS = (
     "s512_segsort_i32", "s512_segsort_f64", "s512_segsort_kv_i32", "s512_segsort_tune",
     "s512_segsort_plan_create", "s512_segsort_plan_launch", "s512_segsort_plan_destroy",
     "s512_learned_root_grad", "s512_learned_fit",
+    "s512_sort_i64", "s512_sort_kv_pairs_i32",
 )
 
 DTYPE_I32, DTYPE_F64, DTYPE_KV_I32 = 0, 1, 2
@@ -137,6 +138,8 @@ def lib() -> ctypes.CDLL:
     L.s512_partition_f64.argtypes = [vp, sz, sz, ctypes.c_double, szp, ci, vp]
     L.s512_partition_kv_i32.argtypes = [vp, vp, sz, sz, ctypes.c_int, szp, ci, vp]
     L.s512_sort_kv_i32.argtypes = [vp, vp, sz, ci, vp]
+    L.s512_sort_i64.argtypes = [vp, sz, ci, vp]
+    L.s512_sort_kv_pairs_i32.argtypes = [vp, sz, ci, vp]
     L.s512_smallsort_kv_i32.argtypes = [vp, vp, sz, ci, vp]
     L.s512_core_small_sort_kv_i32.argtypes = [vp, vp, ci, ci, vp]
     L.s512_popcount.argtypes = [ctypes.c_uint]
@@ -172,7 +175,7 @@ def _ptr(a):
     import torch  # noqa: F401  (torch tensors only)
     if not a.is_contiguous():
         raise ValueError("tensor must be contiguous")
-    name = {"torch.int32": "int32", "torch.float64": "float64"}[str(a.dtype)]
+    name = {"torch.int32": "int32", "torch.float64": "float64", "torch.int64": "int64"}[str(a.dtype)]
     return a.data_ptr(), a.numel(), name, a.is_cuda
 
 
@@ -193,15 +196,28 @@ def _suffix(dt: str) -> str:
         return "i32"
     if dt == "float64":
         return "f64"
+    if dt == "int64":
+        return "i64"
     raise TypeError(f"unsupported dtype {dt}")
 
 
 # -- Sort512 ------------------------------------------------------------------
 def sort(a, flags: int = 0, stream=None) -> None:
-    """Sort512::Sort: in-place ascending sort of int32 / float64 data."""
+    """Sort512::Sort: in-place ascending sort of int32 / float64 / int64 data."""
     p, n, dt, dev = _ptr(a)
     fn = f"s512_sort_{_suffix(dt)}"
     _check(fn, getattr(lib(), fn)(p, n, _flags(dev, flags), _stream(stream)))
+
+
+def sort_pairs(a, flags: int = 0, stream=None) -> None:
+    """Sort512kv::Sort on int[2] pairs (key, value) stored interleaved: an
+    int32 array of shape (n, 2), sorted by key, then value."""
+    if tuple(a.shape[1:]) != (2,):
+        raise ValueError("pairs must have shape (n, 2)")
+    p, n, dt, dev = _ptr(a)
+    if dt != "int32":
+        raise TypeError("pairs must be int32")
+    _check("s512_sort_kv_pairs_i32", lib().s512_sort_kv_pairs_i32(p, n // 2, _flags(dev, flags), _stream(stream)))
 
 
 def small_sort(a, flags: int = 0, stream=None) -> None:

@@ -121,6 +121,15 @@ S512_API int s512_sort_f64(double* data, size_t n, int flags, void* stream);
  *     sort512kv.hpp:6132-6136 (and SortOmpPartition, sort512kv.hpp:6165) */
 S512_API int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream);
 
+/* --- 64-bit words the reference names but does not implement:
+ *     int key/value pairs stored interleaved, pairs[2i] = key, pairs[2i+1] =
+ *     value (the "int[2]" of the reference's README.md:6; its kv interface,
+ *     Sort512kv::Sort at sort512kv.hpp:6133-6163, takes two arrays), sorted by
+ *     (key, value); and int64 keys (no counterpart in the reference, which
+ *     sorts int and double only).  Same pipeline and flags as above. */
+S512_API int s512_sort_kv_pairs_i32(int* pairs, size_t n, int flags, void* stream);
+S512_API int s512_sort_i64(long long* data, size_t n, int flags, void* stream);
+
 /* --- Sort512::Partition512<IndexType>(array, left, right, pivot)
  *     int sort512.hpp:5729-5819, double 5821-5912; kv sort512kv.hpp:5959-6082.
  *     Inclusive range [left, right]; elements <= pivot first.  *boundary

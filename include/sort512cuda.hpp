@@ -61,6 +61,12 @@ inline void check(const char* fn, int rc) {
 }
 inline int call(int* a, size_t n, int flags, void* st) { return s512_sort_i32(a, n, flags, st); }
 inline int call(double* a, size_t n, int flags, void* st) { return s512_sort_f64(a, n, flags, st); }
+// 64-bit integer keys (an extension: the reference sorts int and double)
+inline int call(long long* a, size_t n, int flags, void* st) { return s512_sort_i64(a, n, flags, st); }
+inline int call(long* a, size_t n, int flags, void* st) {
+    static_assert(sizeof(long) == sizeof(long long), "64-bit long expected");
+    return s512_sort_i64(reinterpret_cast<long long*>(a), n, flags, st);
+}
 }  // namespace detail
 
 // Tag for explicit device pointers (no pointer probe, optional async stream).
@@ -262,6 +268,20 @@ inline void Sort(DevicePtr<SortType> array, DevicePtr<SortType> values, const In
 template <class SortType, class IndexType = size_t>
 inline void SortOmpPartition(SortType array[], SortType values[], const IndexType size) {
     Sort<SortType, IndexType>(array, values, size);
+}
+
+// int[2] pairs (key, value) stored interleaved, as the reference's README
+// describes its kv sort; sorted by key, then value.
+template <class IndexType = size_t>
+inline void Sort(int (*pairs)[2], const IndexType size) {
+    Sort512::detail::check("Sort512kv::Sort", s512_sort_kv_pairs_i32(&pairs[0][0], (size_t)size, S512_PTR_AUTO, nullptr));
+}
+
+template <class IndexType = size_t>
+inline void Sort(DevicePtr<int[2]> pairs, const IndexType size, cudaStream_t stream = nullptr, bool async = false) {
+    Sort512::detail::check("Sort512kv::Sort",
+                           s512_sort_kv_pairs_i32(&pairs.ptr[0][0], (size_t)size,
+                                                  S512_PTR_DEVICE | (async ? S512_ASYNC : 0), stream));
 }
 
 template <class IndexType>

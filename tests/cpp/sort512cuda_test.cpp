@@ -333,6 +333,36 @@ static void test_parallel_merge() {
     }
 }
 
+// Extensions: 64-bit integer keys and interleaved int[2] pairs.
+static void test_wide_words() {
+    std::printf("Sort<long long>, Sort512kv::Sort(int[2])\n");
+    for (size_t n : {size_t(1), size_t(100), size_t(5000), size_t(300000)}) {
+        std::vector<long long> a(n);
+        for (size_t i = 0; i < n; ++i)
+            a[i] = (long long)((drand48() - 0.5) * 9.0e18);
+        std::vector<long long> want(a);
+        std::sort(want.begin(), want.end());
+        Sort512::Sort<long long, size_t>(a.data(), n);
+        assert_equal(a.data(), want.data(), n, "Sort<long long>");
+
+        std::vector<int> p(2 * n);
+        for (size_t i = 0; i < n; ++i) {
+            p[2 * i] = int(drand48() * double(n / 4 + 1)) - int(n / 8);
+            p[2 * i + 1] = int(drand48() * 2.0e9) - 1000000000;
+        }
+        std::vector<std::pair<int, int>> wp(n);
+        for (size_t i = 0; i < n; ++i) wp[i] = {p[2 * i], p[2 * i + 1]};
+        std::sort(wp.begin(), wp.end());
+        Sort512kv::Sort(reinterpret_cast<int(*)[2]>(p.data()), n);
+        for (size_t i = 0; i < n; ++i)
+            if (p[2 * i] != wp[i].first || p[2 * i + 1] != wp[i].second) {
+                std::printf("pairs differ at %zu (n=%zu)\n", i, n);
+                g_fail = 1;
+                break;
+            }
+    }
+}
+
 int main() {
     test_popcount();
     test_sort_nvec<int, 16>();
@@ -349,6 +379,7 @@ int main() {
     test_partition_pair();
     test_parallel_merge<int>();
     test_parallel_merge<double>();
+    test_wide_words();
     if (g_fail) std::printf("Test failed!\n");
     else std::printf("All tests passed\n");
     return g_fail;
