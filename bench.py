@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--n", type=int, default=N_KEYS)
     ap.add_argument("--no-extras", action="store_true", help="skip the per-distribution / int32 / kv extras")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--sharded", action="store_true",
+                    help="with --gpus N > 1: one sorted array across the ranks (sample sort with one "
+                         "all-to-all) instead of N independent sorts")
     return ap.parse_args()
 
 
@@ -349,6 +352,57 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_sharded(args, world, rank, local):
+    """--sharded: each rank holds n doubles of one array; the sort across
+    ranks (dist_sort.sort_sharded: local sort, regular sample, splitters, one
+    all-to-all over NCCL, merge of the received runs) is timed on the device,
+    max over ranks.  value = n * N / time (weak scaling)."""
+    import torch
+
+    import dist_sort
+    import sort512cuda as s512
+    import workloads
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    s512.lib()
+    n = args.n
+    stream = torch.cuda.current_stream(dev)
+
+    def make(seed):
+        return workloads.uniform01_torch(n, seed=seed + 7919 * rank, device=dev)
+
+    for w in range(args.warmup):
+        dist_sort.sort_sharded(make(900 + w))
+    torch.cuda.synchronize()
+    inputs = [make(s) for s in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    out = None
+    for s in range(args.steps):
+        out = dist_sort.sort_sharded(inputs[s])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    outs_ok = bool((out[1:] >= out[:-1]).all()) if out is not None and out.numel() > 1 else True
+    del out
+    barrier(world)
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world) / args.steps
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": round(n * world / (ms * 1e-3) / 1e9, 3), "unit": "Gkeys/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "one array of n doubles per rank, sorted across the ranks", "n_per_rank": n,
+                   "parallelism": f"sample sort over {world} ranks (one all-to-all)"},
+        "sorted_ok": outs_ok, "e2e": None, "roofline": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def _timed(fn, stream):
     import torch
     e0 = torch.cuda.Event(enable_timing=True)
@@ -588,6 +642,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, world, rank)
+        elif args.sharded and world > 1:
+            run_sharded(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
