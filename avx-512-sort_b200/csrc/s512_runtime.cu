@@ -14,7 +14,7 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 
-static s512_config g_cfg = {S512_SPLIT_PLAIN, 0, 3.0, 0x5EEDull, 0};
+static s512_config g_cfg = {S512_SPLIT_PLAIN, 0, 3.0, 0x5EEDull, 0, 0};
 s512_config& config() { return g_cfg; }
 
 static thread_local s512_stats g_stats;

@@ -12,6 +12,7 @@
 // host (the level's item counts and error word).
 #include "s512_pipeline.cuh"
 #include "s512_partition2.cuh"
+#include "s512_stream.cuh"
 
 using namespace s512;
 
@@ -30,6 +31,11 @@ int s512_sort_i32(int* data, size_t n, int flags, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
     const bool host = pointer_kind(data, flags) == 1;
+    if (host && stream_needed(n, sizeof(int))) {  // larger than the device budget
+        int rc = stream_sort<int>(*C, data, n, st);
+        if (rc) return rc;
+        return finish_call(guard_, st, flags, host);
+    }
     int* d = data;
     if (host) {
         d = (int*)C->get("stage0", n * sizeof(int));
@@ -48,6 +54,11 @@ int s512_sort_f64(double* data, size_t n, int flags, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
     const bool host = pointer_kind(data, flags) == 1;
+    if (host && stream_needed(n, sizeof(double))) {  // larger than the device budget
+        int rc = stream_sort<double>(*C, data, n, st);
+        if (rc) return rc;
+        return finish_call(guard_, st, flags, host);
+    }
     unsigned long long* d = (unsigned long long*)data;
     if (host) {
         d = (unsigned long long*)C->get("stage0", n * sizeof(double));

@@ -4,6 +4,9 @@
 // its kv interface, sort512kv.hpp:6133, takes two separate arrays).  Same
 // pipeline as s512_sort.cu, through the CodecI64 / CodecKVPairs codecs.
 #include "s512_pipeline.cuh"
+#include "s512_stream.cuh"
+
+#include <type_traits>
 
 using namespace s512;
 
@@ -19,6 +22,13 @@ static int sort_words(T* data, size_t n, int flags, void* stream) {
     if (!C) return status;
     CallGuard guard(C, st);
     const bool host = pointer_kind(data, flags) == 1;
+    if constexpr (std::is_same<Codec, CodecI64>::value) {
+        if (host && stream_needed(n, 8)) {  // larger than the device budget
+            int rc = stream_sort<long long>(*C, data, n, st);
+            if (rc) return rc;
+            return finish_call(guard, st, flags, host);
+        }
+    }
     unsigned long long* d = (unsigned long long*)data;
     if (host) {
         d = (unsigned long long*)C->get("stage0", n * 8);

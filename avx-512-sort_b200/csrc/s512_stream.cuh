@@ -1,0 +1,181 @@
+// s512_stream.cuh -- host arrays larger than the device budget: an external
+// sort streamed through the device in two passes over PCIe.
+//
+// The reference sorts host memory of any size in place (Sort512::Sort on a
+// host array; its benchmark goes to 2^30 keys, sort512perf.cpp:374).  A host
+// array whose sort would not fit the device budget (s512_config.device_budget,
+// about six times the data for the array plus the level buffers) is sorted
+// here as:
+//   1. runs: consecutive pieces of m keys are copied in, sorted on the device
+//      and copied out to a pinned staging array;
+//   2. merge by exact rank: output piece j holds ranks [j*m, (j+1)*m).  For
+//      each boundary rank the host finds the boundary key by bisection over
+//      the encoded key range (counting keys <= a value with one binary search
+//      per run) and splits ties between runs in run order, which gives every
+//      run's cut exactly; piece j is then the runs' slices between two cuts,
+//      gathered to the device, sorted there and copied to its final place in
+//      the caller's array.
+// Every piece holds at most m keys whatever the data (ties included), so the
+// device budget holds.  Keys cross PCIe twice each way.
+#pragma once
+
+#include <cstring>
+#include <vector>
+
+#include "s512_pipeline.cuh"
+
+namespace s512 {
+
+// Host-side order-preserving encodings, the same transforms as the device
+// codecs (s512_common.cuh).
+inline uint64_t host_key(int x) { return (uint32_t)x ^ 0x80000000u; }
+inline uint64_t host_key(long long x) { return (uint64_t)x ^ 0x8000000000000000ull; }
+inline uint64_t host_key(double x) {
+    uint64_t u;
+    std::memcpy(&u, &x, 8);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+template <typename T> struct StreamTypes;
+template <> struct StreamTypes<int> {
+    using K = uint32_t;
+    static CodecI32 codec(void* d) { return CodecI32{(const int*)d, (int*)d}; }
+};
+template <> struct StreamTypes<double> {
+    using K = uint64_t;
+    static CodecF64 codec(void* d) {
+        return CodecF64{(const unsigned long long*)d, (unsigned long long*)d};
+    }
+};
+template <> struct StreamTypes<long long> {
+    using K = uint64_t;
+    static CodecI64 codec(void* d) {
+        return CodecI64{(const unsigned long long*)d, (unsigned long long*)d};
+    }
+};
+
+// Device bytes one host-pointer call may use.
+inline size_t device_budget() {
+    if (config().device_budget) return (size_t)config().device_budget;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return (size_t)1 << 34;
+    }
+    return free_b / 10 * 8;
+}
+
+// Keys per streamed piece: the piece, its level buffers and scratch in ~6x.
+inline size_t stream_piece_keys(size_t esz) {
+    size_t m = device_budget() / (6 * esz);
+    m &= ~(size_t)4095;
+    return m < 65536 ? 65536 : m;
+}
+
+inline bool stream_needed(size_t n, size_t esz) { return n > stream_piece_keys(esz); }
+
+// Number of keys of the sorted run r[0..len) whose encoded key is <= v (or < v).
+template <typename T>
+static size_t count_le(const T* r, size_t len, uint64_t v, bool strict) {
+    size_t lo = 0, hi = len;
+    while (lo < hi) {
+        const size_t mid = lo + (hi - lo) / 2;
+        const uint64_t k = host_key(r[mid]);
+        if (strict ? k < v : k <= v) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+template <typename T>
+static int stream_sort(DevCtx& C, T* host, size_t n, cudaStream_t st) {
+    using ST = StreamTypes<T>;
+    using K = typename ST::K;
+    const size_t esz = sizeof(T);
+    const size_t m = stream_piece_keys(esz);
+    const size_t nruns = (n + m - 1) / m;
+
+    struct Pinned {
+        T* p = nullptr;
+        ~Pinned() {
+            if (p) cudaFreeHost(p);
+        }
+    } stage;
+    if (cudaMallocHost((void**)&stage.p, n * esz) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMallocHost of %zu bytes for the streamed sort failed", n * esz);
+        return S512_ERR_ALLOC;
+    }
+    T* d = (T*)C.get("stream_piece", m * esz);
+    if (!d) return S512_ERR_ALLOC;
+
+    // 1. sorted runs of m keys into the staging array
+    for (size_t r = 0; r < nruns; ++r) {
+        const size_t off = r * m, len = (n - off) < m ? (n - off) : m;
+        S512_CUDA_TRY(cudaMemcpyAsync(d, host + off, len * esz, cudaMemcpyHostToDevice, st));
+        int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
+        if (rc) return rc;
+        S512_CUDA_TRY(cudaMemcpyAsync(stage.p + off, d, len * esz, cudaMemcpyDeviceToHost, st));
+    }
+    S512_CUDA_TRY(cudaStreamSynchronize(st));
+
+    auto run_ptr = [&](size_t r) { return stage.p + r * m; };
+    auto run_len = [&](size_t r) { return (n - r * m) < m ? (n - r * m) : m; };
+
+    // 2. cuts at ranks j*m: cut[j][r] = keys of run r that go before rank j*m
+    std::vector<std::vector<size_t>> cut(nruns + 1, std::vector<size_t>(nruns, 0));
+    for (size_t r = 0; r < nruns; ++r) cut[nruns][r] = run_len(r);
+    uint64_t kmin = ~0ull, kmax = 0;
+    for (size_t r = 0; r < nruns; ++r) {
+        const uint64_t a = host_key(run_ptr(r)[0]), b = host_key(run_ptr(r)[run_len(r) - 1]);
+        kmin = a < kmin ? a : kmin;
+        kmax = b > kmax ? b : kmax;
+    }
+    for (size_t j = 1; j < nruns; ++j) {
+        const size_t rank = j * m;
+        // smallest encoded v with (keys <= v) >= rank
+        uint64_t lo = kmin, hi = kmax;
+        while (lo < hi) {
+            const uint64_t mid = lo + (hi - lo) / 2;
+            size_t c = 0;
+            for (size_t r = 0; r < nruns; ++r) c += count_le(run_ptr(r), run_len(r), mid, false);
+            if (c >= rank) hi = mid; else lo = mid + 1;
+        }
+        const uint64_t v = lo;
+        size_t below = 0;
+        std::vector<size_t> lt(nruns), le(nruns);
+        for (size_t r = 0; r < nruns; ++r) {
+            lt[r] = count_le(run_ptr(r), run_len(r), v, true);
+            le[r] = count_le(run_ptr(r), run_len(r), v, false);
+            below += lt[r];
+        }
+        size_t need = rank - below;  // keys equal to v that go before the cut, taken in run order
+        for (size_t r = 0; r < nruns; ++r) {
+            const size_t take = (le[r] - lt[r]) < need ? (le[r] - lt[r]) : need;
+            cut[j][r] = lt[r] + take;
+            need -= take;
+        }
+    }
+
+    // 3. each output piece: gather its slices, sort, copy to its final place
+    for (size_t j = 0; j < nruns; ++j) {
+        size_t len = 0;
+        for (size_t r = 0; r < nruns; ++r) {
+            const size_t a = cut[j][r], b = cut[j + 1][r];
+            if (b > a) {
+                S512_CUDA_TRY(cudaMemcpyAsync(d + len, run_ptr(r) + a, (b - a) * esz, cudaMemcpyHostToDevice, st));
+                len += b - a;
+            }
+        }
+        if (len != run_len(j)) {
+            set_error("streamed sort: piece %zu holds %zu keys, expected %zu", j, len, run_len(j));
+            return S512_ERR_INTERNAL;
+        }
+        int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
+        if (rc) return rc;
+        S512_CUDA_TRY(cudaMemcpyAsync(host + j * m, d, len * esz, cudaMemcpyDeviceToHost, st));
+    }
+    S512_CUDA_TRY(cudaStreamSynchronize(st));
+    return S512_OK;
+}
+
+}  // namespace s512

@@ -55,7 +55,8 @@ DTYPE_I32, DTYPE_F64, DTYPE_KV_I32 = 0, 1, 2
 
 class Config(ctypes.Structure):
     _fields_ = [("splitter_mode", ctypes.c_int), ("collect_stats", ctypes.c_int),
-                ("max_imbalance", ctypes.c_double), ("seed", ctypes.c_uint64), ("fault_inject", ctypes.c_int)]
+                ("max_imbalance", ctypes.c_double), ("seed", ctypes.c_uint64), ("fault_inject", ctypes.c_int),
+                ("device_budget", ctypes.c_uint64)]
 
 
 FAULT_OVERFLOW, FAULT_REJECT_MODEL, FAULT_ALLOC, FAULT_TIMEOUT = 1, 2, 4, 8

@@ -68,6 +68,9 @@ typedef struct s512_config {
     double max_imbalance;     /* learned model is rejected if max bucket > this x mean (default 3.0) */
     uint64_t seed;            /* sampling seed (default 0x5EED) */
     int fault_inject;         /* testing only: S512_FAULT_* bits, 0 in normal use */
+    uint64_t device_budget;   /* host-pointer sorts: device bytes one call may use (0: 80% of the free
+                                 memory); a host array larger than the budget allows is sorted in
+                                 pieces streamed through the device (s512_sort_* below) */
 } s512_config;
 
 /* Failure injection (tests of the library's own error paths; 0 by default).
