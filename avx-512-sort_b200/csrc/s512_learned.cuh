@@ -1,7 +1,7 @@
 // s512_learned.cuh -- learned splitters: a small monotone CDF model per
 // segment, fitted on the device to the segment's sorted sample, that maps a
 // key to its bucket in a few arithmetic steps instead of the plain splitters'
-// eight-level tree search.  The plain splitters stay as the fallback.
+// slot table and compares.  The plain splitters stay as the fallback.
 //
 // Model (all slopes non-negative, so the map is monotone by construction):
 //   z   = float(key - kmin) * inv_range                      (saturating at 0)

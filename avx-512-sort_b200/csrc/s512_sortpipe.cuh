@@ -53,6 +53,7 @@ struct SegDesc {
 template <typename K>
 struct SplitSet {
     K tree[NB];            // Eytzinger tree of the unique splitters, nodes 1..255, padded with max
+                           // (the exact-count fallback's search; the pass uses slot_tab)
     K uniq[NB];            // unique splitters in ascending order (padded with max)
     uint64_t region_off[NB];  // bucket region start, relative to SegDesc::out_base
     uint64_t region_cap[NB];  // bucket region capacity (keys)
@@ -626,7 +627,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
             const uint32_t idx = (uint32_t)(r * THREADS + tid);
             if (idx < cnt) key[r] = idx < tma_elems ? in.decode(sm.buf[b], idx, TILE) : in.load(base + idx);
         }
-        // all IPT tree searches first: they are independent chains of shared
+        // all IPT bucket lookups first: they are independent chains of shared
         // loads, so the scheduler can overlap them
         uint32_t bks[IPT];
 #pragma unroll
