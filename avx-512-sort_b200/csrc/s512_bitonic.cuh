@@ -1,5 +1,5 @@
-// s512_bitonic.cuh -- bitonic sorting networks in registers, across a warp
-// with __shfl_xor_sync, and across a block through shared memory.
+// s512_bitonic.cuh -- bitonic sorting networks in registers and across a
+// warp with __shfl_xor_sync.
 //
 // This is the GPU form of the reference's leaf: SmallSort16V (sort512.hpp:
 // 5312-5689 int, 2255-2634 double) loads up to 16 AVX-512 vectors, pads the
@@ -7,9 +7,9 @@
 // min/max + mask blend, e.g. CoreSmallSort 2637-2720, CoreExchangeSort2V
 // 2727-2783, CoreSmallEnd 3873-4813) and stores the first `length` lanes.
 // Here one warp holds 32*IPT keys, IPT per lane in registers; a stage whose
-// partner is in the same lane is a register min/max, a stage whose partner is
-// in another lane is a __shfl_xor_sync exchange, and a stage whose partner is
-// in another warp goes through shared memory.
+// partner is in the same lane is a register min/max, and a stage whose partner
+// is in another lane is a __shfl_xor_sync exchange.  Longer runs are merged
+// (s512_blocksort.cuh).
 //
 // Element layout ("blocked"): lane l of warp w holds elements
 //   e = (w*32 + l)*IPT + r,  r = 0..IPT-1.
@@ -92,38 +92,6 @@ __device__ __forceinline__ void warp_bitonic_sort(K (&x)[IPT]) {
             lane_mirror<K, IPT>(x, k / IPT - 1, k / IPT / 2);
         }
         warp_half_cleaners<K, IPT>(x, k / 4);
-    }
-}
-
-// Cross-warp stage through shared memory: partner e ^ m (m >= 32*IPT for a
-// half-cleaner, or m = k-1 for a mirror).  `hb` is the element bit that marks
-// the upper member of each pair.  smem must hold THREADS*IPT keys.
-template <typename K, int IPT>
-__device__ __forceinline__ void smem_stage(K (&x)[IPT], K* smem, unsigned m, unsigned hb) {
-    const unsigned base = threadIdx.x * IPT;
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) smem[base + r] = x[r];
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < IPT; ++r) {
-        const unsigned e = base + r;
-        const K y = smem[e ^ m];
-        x[r] = keep_side(x[r], y, (e & hb) != 0);
-    }
-    __syncthreads();
-}
-
-// Sort THREADS*IPT keys held by the block (blocked layout), ascending.
-template <typename K, int THREADS, int IPT>
-__device__ __forceinline__ void block_bitonic_sort(K (&x)[IPT], K* smem) {
-    warp_bitonic_sort<K, IPT>(x);
-    constexpr int WARP_N = 32 * IPT;
-#pragma unroll 1
-    for (int k = 2 * WARP_N; k <= THREADS * IPT; k <<= 1) {
-        smem_stage<K, IPT>(x, smem, (unsigned)(k - 1), (unsigned)(k >> 1));
-        int j = k / 4;
-        for (; j >= WARP_N; j >>= 1) smem_stage<K, IPT>(x, smem, (unsigned)j, (unsigned)j);
-        warp_half_cleaners<K, IPT>(x, WARP_N / 2);
     }
 }
 
