@@ -319,72 +319,91 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
         for (int q = lp + 1; q <= l; ++q) leaf_first[q] = i;  // leaves lp+1..l start at i
     }
     __syncthreads();
-    if (tid < LR_LEAVES) {
-        const int l = tid;
-        const uint32_t f = leaf_first[l];
-        // leaf_first[q] = first sample routed to a leaf >= q, so leaf l owns
-        // the samples [leaf_first[l], leaf_first[l+1])
-        const uint32_t e = leaf_first[l + 1];
-        LeafParam<K> P;
-        if (f < e && f < m) {
-            const K base = smp[f];
-            const K span = smp[e - 1] - base;
-            const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
-            // least squares on (u, y), u in [0, 1]
-            float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
-            const float cnt = (float)(e - f);
-            for (uint32_t i = f; i < e; ++i) {
-                const float u = key_to_float(smp[i] - base) * inv_span;
-                const float y = ((float)i + 0.5f) / (float)m;
-                su += u;
-                sy += y;
-                suu += u * u;
-                suy += u * y;
-            }
-            const float mu = su / cnt, my = sy / cnt;
-            const float var = suu / cnt - mu * mu, cov = suy / cnt - mu * my;
-            float b = var > 1e-12f ? cov / var : 0.f;
-            b = b > 0.f ? b : 0.f;
-            float a = my - b * mu;
-            // refine (a, beta), b = beta^2, by Adam on the leaf's squared
-            // error (forward + backward per step); keep the best pair seen
-            float beta = sqrtf(b);
-            float best_a = a, best_beta = beta, best_l = 3.4e38f;
-            Adam oa, ob;
-            for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
-                float ga = 0.f, gb = 0.f, l2 = 0.f;
-                for (uint32_t i = f; i < e; ++i) {
+    // one warp per leaf at a time: the lanes stride over the leaf's
+    // (contiguous) samples and every sum is reduced across the warp and taken
+    // from lane 0, so all lanes step the same parameters.  (A leaf can own
+    // most of the sample when the root is skewed; one thread per leaf would
+    // then walk it alone, once per step.)
+    {
+        const int lane = tid & 31, wid = tid >> 5, nw = (int)(blockDim.x >> 5);
+        auto wsum = [&](float v) {
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
+            return __shfl_sync(0xFFFFFFFFu, v, 0);
+        };
+        for (int l = wid; l < LR_LEAVES; l += nw) {
+            const uint32_t f = leaf_first[l];
+            // leaf_first[q] = first sample routed to a leaf >= q, so leaf l owns
+            // the samples [leaf_first[l], leaf_first[l+1])
+            const uint32_t e = leaf_first[l + 1];
+            LeafParam<K> P;
+            if (f < e && f < m) {
+                const K base = smp[f];
+                const K span = smp[e - 1] - base;
+                const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
+                // least squares on (u, y), u in [0, 1]
+                float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
+                const float cnt = (float)(e - f);
+                for (uint32_t i = f + lane; i < e; i += 32) {
                     const float u = key_to_float(smp[i] - base) * inv_span;
-                    const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
-                    l2 += r * r;
-                    ga += r;
-                    gb += r * u;
+                    const float y = ((float)i + 0.5f) / (float)m;
+                    su += u;
+                    sy += y;
+                    suu += u * u;
+                    suy += u * y;
                 }
-                if (l2 < best_l) {
-                    best_l = l2;
-                    best_a = a;
-                    best_beta = beta;
+                su = wsum(su);
+                sy = wsum(sy);
+                suu = wsum(suu);
+                suy = wsum(suy);
+                const float mu = su / cnt, my = sy / cnt;
+                const float var = suu / cnt - mu * mu, cov = suy / cnt - mu * my;
+                float b = var > 1e-12f ? cov / var : 0.f;
+                b = b > 0.f ? b : 0.f;
+                float a = my - b * mu;
+                // refine (a, beta), b = beta^2, by Adam on the leaf's squared
+                // error (forward + backward per step); keep the best pair seen
+                float beta = sqrtf(b);
+                float best_a = a, best_beta = beta, best_l = 3.4e38f;
+                Adam oa, ob;
+                for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
+                    float ga = 0.f, gb = 0.f, l2 = 0.f;
+                    for (uint32_t i = f + lane; i < e; i += 32) {
+                        const float u = key_to_float(smp[i] - base) * inv_span;
+                        const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
+                        l2 += r * r;
+                        ga += r;
+                        gb += r * u;
+                    }
+                    l2 = wsum(l2);
+                    ga = wsum(ga);
+                    gb = wsum(gb);
+                    if (l2 < best_l) {
+                        best_l = l2;
+                        best_a = a;
+                        best_beta = beta;
+                    }
+                    if (it > LR_LEAF_ITERS) break;
+                    ga *= 2.f / cnt;
+                    gb *= 2.f / cnt * 2.f * beta;
+                    a -= oa.step(ga, LR_STEP / (float)m, it);
+                    beta -= ob.step(gb, LR_STEP / (float)m, it);
                 }
-                if (it > LR_LEAF_ITERS) break;
-                ga *= 2.f / cnt;
-                gb *= 2.f / cnt * 2.f * beta;
-                a -= oa.step(ga, LR_STEP / (float)m, it);
-                beta -= ob.step(gb, LR_STEP / (float)m, it);
+                a = best_a;
+                beta = best_beta;
+                P.base = base;
+                P.a = a;
+                P.b = beta * beta * inv_span;  // slope per unit of (key - base)
+                P.lo = ((float)f + 0.5f) / (float)m;
+                P.hi = ((float)(e - 1) + 0.5f) / (float)m;
+            } else {
+                P.base = KeyMax<K>::value;
+                P.a = 0.f;
+                P.b = 0.f;
+                P.lo = P.hi = -1.f;  // patched below: an empty leaf repeats its left neighbour's top
             }
-            a = best_a;
-            beta = best_beta;
-            P.base = base;
-            P.a = a;
-            P.b = beta * beta * inv_span;  // slope per unit of (key - base)
-            P.lo = ((float)f + 0.5f) / (float)m;
-            P.hi = ((float)(e - 1) + 0.5f) / (float)m;
-        } else {
-            P.base = KeyMax<K>::value;
-            P.a = 0.f;
-            P.b = 0.f;
-            P.lo = P.hi = -1.f;  // patched below: an empty leaf repeats its left neighbour's top
+            if (lane == 0) L.leaf[l] = P;
         }
-        L.leaf[l] = P;
     }
     __syncthreads();
     if (tid == 0) {
