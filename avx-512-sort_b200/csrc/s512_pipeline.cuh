@@ -14,8 +14,8 @@ template <typename K> struct PartShape;
 template <> struct PartShape<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
 template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT = 8; };
 template <typename K> struct PartShapeOne;
-template <> struct PartShapeOne<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
-template <> struct PartShapeOne<uint64_t> { static constexpr int THREADS = 1024, IPT = 8; };
+template <> struct PartShapeOne<uint32_t> { static constexpr int THREADS = 1024, IPT = 16; };
+template <> struct PartShapeOne<uint64_t> { static constexpr int THREADS = 1024, IPT = 12; };
 
 // ---------------------------------------------------------------------------
 // leaf launches per class
