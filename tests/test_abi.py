@@ -64,3 +64,31 @@ def test_no_cpu_fallback_in_product():
             if f.endswith((".cu", ".cuh", ".py", ".hpp", ".h")):
                 text = open(os.path.join(dirpath, f)).read()
                 assert "oracle" not in text.lower(), f
+
+
+def test_arguments_checked_before_any_device_work(s512):
+    lib = s512.lib()
+    assert lib.s512_sort_i32(None, 10, 0, None) == s512.S512_ERR_ARG
+    assert lib.s512_sort_f64(None, 10, 0, None) == s512.S512_ERR_ARG
+    assert lib.s512_sort_i64(None, 10, 0, None) == s512.S512_ERR_ARG
+    assert lib.s512_sort_kv_pairs_i32(None, 10, 0, None) == s512.S512_ERR_ARG
+    a = (ctypes.c_int * 4)()
+    assert lib.s512_sort_kv_i32(a, None, 4, 0, None) == s512.S512_ERR_ARG
+    # an empty array is a no-op (undefined in the reference)
+    assert lib.s512_sort_i32(None, 0, 0, None) == 0
+    assert lib.s512_sort_f64(None, 0, 0, None) == 0
+
+
+def test_no_device_fails_loudly(s512):
+    # without a B200 the library reports it and leaves the data untouched: no
+    # host fallback sorts behind the caller's back
+    import torch
+    if torch.cuda.is_available():
+        import pytest
+        pytest.skip("a GPU is present")
+    import numpy as np
+    a = np.arange(100, dtype=np.int32)[::-1].copy()
+    rc = s512.lib().s512_sort_i32(a.ctypes.data, a.size, 0, None)
+    assert rc == s512.S512_ERR_UNSUPPORTED
+    assert s512.lib().s512_last_error_string()
+    assert np.array_equal(a, np.arange(100, dtype=np.int32)[::-1])
