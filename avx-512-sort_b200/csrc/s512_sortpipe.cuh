@@ -87,14 +87,15 @@ struct LeafItem {
 // Leaf size classes.  Class 0 is one warp per bucket (a 256-key bitonic
 // leaf); the others are one block per bucket (the slot sort of
 // s512_slotsort.cuh, with the bitonic + merge-path block sort for uneven
-// buckets).  A bucket's class is the smallest that holds it, so its keys fill
-// between 2/3 and all of the class's slots above 4096.  The copy list holds
-// equality buckets.
-constexpr int NCLASS = 7;
+// buckets).  A bucket's class is the smallest that holds it; the classes
+// above 4096 are close together, because small blocks sort their keys faster
+// (more buckets in flight per SM) and a bucket's keys should fill most of its
+// class's slots.  The copy list holds equality buckets.
+constexpr int NCLASS = 8;
 constexpr int CLS_COPY = NCLASS;  // index of the copy list
 __host__ __device__ constexpr int class_cap(int c) {
-    // 256 | 1024 2048 4096 6144 8192 16384
-    return c == 0 ? 256 : c == 4 ? 6144 : (c < 4 ? (512 << c) : (512 << (c - 1)));
+    return c == 0 ? 256 : c == 1 ? 1024 : c == 2 ? 2048 : c == 3 ? 4096 : c == 4 ? 4608 : c == 5 ? 6144
+         : c == 6 ? 8192 : 16384;
 }
 __host__ __device__ constexpr uint32_t leaf_max(int /*key_bytes*/) { return 16384u; }
 __host__ __device__ inline int class_of(int /*key_bytes*/, uint32_t count) {
@@ -1018,7 +1019,9 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
 
 // Blocks per SM that the leaf kernel's register budget is sized for (the
 // 384-thread class fits three, with its keys' shared memory unpadded).
-__host__ __device__ constexpr int leaf_min_blocks(int threads) { return threads == 384 ? 3 : 1024 / threads; }
+__host__ __device__ constexpr int leaf_min_blocks(int threads) {
+    return (threads == 288 || threads == 384) ? 3 : 1024 / threads;
+}
 
 // One block per bucket of at most THREADS*EPT keys: distribution counting
 // into value slots (s512_slotsort.cuh).  The next bucket's keys are loaded
