@@ -63,9 +63,10 @@ static int launch_leaf_class(DevCtx& C, int cls, const LeafItem<K>* items, uint3
         case 2: return launch_leaf_block<K, OutCodec, 256, 8>(C, items, n, out, uneven, n_uneven, st);
         case 3: return launch_leaf_block<K, OutCodec, 256, 16>(C, items, n, out, uneven, n_uneven, st);
         case 4: return launch_leaf_block<K, OutCodec, 288, 16>(C, items, n, out, uneven, n_uneven, st);
-        case 5: return launch_leaf_block<K, OutCodec, 384, 16>(C, items, n, out, uneven, n_uneven, st);
-        case 6: return launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, uneven, n_uneven, st);
-        case 7: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 5: return launch_leaf_block<K, OutCodec, 320, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 6: return launch_leaf_block<K, OutCodec, 384, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 7: return launch_leaf_block<K, OutCodec, 512, 16>(C, items, n, out, uneven, n_uneven, st);
+        case 8: return launch_leaf_block<K, OutCodec, 1024, 16>(C, items, n, out, uneven, n_uneven, st);
         case CLS_COPY: {
             auto fn = leaf_copy_kernel<K, OutCodec>;
             int grid = 0;
@@ -105,7 +106,8 @@ static int sort_one_leaf(DevCtx& C, InCodec in, OutCodec out, uint32_t n, cudaSt
         case 3: return launch_small_block<InCodec, OutCodec, 512, 8>(C, in, out, n, st);
         case 4:
         case 5:
-        case 6: return launch_small_block<InCodec, OutCodec, 512, 16>(C, in, out, n, st);
+        case 6:
+        case 7: return launch_small_block<InCodec, OutCodec, 512, 16>(C, in, out, n, st);
         default: return launch_small_block<InCodec, OutCodec, 1024, 16>(C, in, out, n, st);
     }
 }

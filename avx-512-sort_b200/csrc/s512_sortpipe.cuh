@@ -91,11 +91,11 @@ struct LeafItem {
 // above 4096 are close together, because small blocks sort their keys faster
 // (more buckets in flight per SM) and a bucket's keys should fill most of its
 // class's slots.  The copy list holds equality buckets.
-constexpr int NCLASS = 8;
+constexpr int NCLASS = 9;
 constexpr int CLS_COPY = NCLASS;  // index of the copy list
 __host__ __device__ constexpr int class_cap(int c) {
-    return c == 0 ? 256 : c == 1 ? 1024 : c == 2 ? 2048 : c == 3 ? 4096 : c == 4 ? 4608 : c == 5 ? 6144
-         : c == 6 ? 8192 : 16384;
+    return c == 0 ? 256 : c == 1 ? 1024 : c == 2 ? 2048 : c == 3 ? 4096 : c == 4 ? 4608 : c == 5 ? 5120
+         : c == 6 ? 6144 : c == 7 ? 8192 : 16384;
 }
 __host__ __device__ constexpr uint32_t leaf_max(int /*key_bytes*/) { return 16384u; }
 __host__ __device__ inline int class_of(int /*key_bytes*/, uint32_t count) {
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(256) leaf_warp_kernel(const LeafItem<K>* __res
 // Blocks per SM that the leaf kernel's register budget is sized for (the
 // 384-thread class fits three, with its keys' shared memory unpadded).
 __host__ __device__ constexpr int leaf_min_blocks(int threads) {
-    return (threads == 288 || threads == 384) ? 3 : 1024 / threads;
+    return (threads == 288 || threads == 320 || threads == 384) ? 3 : 1024 / threads;
 }
 
 // One block per bucket of at most THREADS*EPT keys: distribution counting
