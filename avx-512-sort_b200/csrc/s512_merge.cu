@@ -71,7 +71,7 @@ static int merge_entry(T* data, size_t n, size_t middle, int flags, void* stream
     DevCtx* C = current_ctx(&status);
     if (!C) return status;
     CallGuard guard(C, st);
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     T* d = data;
     if (host) {
         d = (T*)C->get("stage0", n * sizeof(T));
@@ -101,7 +101,7 @@ static int sort_by_chunks(T* data, size_t n, int nparts, int flags, void* stream
     int status = S512_OK;
     DevCtx* C = current_ctx(&status);
     if (!C) return status;
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     T* d = data;
     if (host) {
         CallGuard g(C, st);

@@ -18,9 +18,17 @@
 //     contents; this file clears what must start at zero on every call, and
 //     calls whose work overlaps on the GPU (different streams, or threads that
 //     do not wait for each other) race on it;
-//   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//   * the first call on a device does the set-up: with that device current it
+//     looks up the array's device address (cudaGetSymbolAddress) and the
+//     kernel's occupancy.  CUDA loads modules lazily by default
+//     (CUDA_MODULE_LOADING=LAZY), so that first call is also when the driver
+//     loads this file's module and reserves the array's memory on the device.
+//     Make it at start-up, before another allocator takes the device's memory
+//     and before any stream capture; a call with an empty range (right < left)
+//     does only this set-up;
+//   * `data` must be memory of the current device (or managed memory);
+//   * the partitioned range is copied back over the caller's data only when
+//     the kernel reports no error, so a failed call leaves the data as it was.
 #include <mutex>
 
 #include "s512_partition2.cuh"
@@ -36,7 +44,9 @@ constexpr size_t NA_TILES = (NA_MAX + NA_TILE - 1) / NA_TILE;
 // [keys: NA_MAX ints][status: NA_TILES x 2 words][control block]
 constexpr size_t NA_KEYS_BYTES = NA_MAX * sizeof(int);
 constexpr size_t NA_STATUS_OFF = NA_KEYS_BYTES;
-constexpr size_t NA_STATUS_BYTES = NA_TILES * 2 * sizeof(unsigned long long);
+// (one spare pair of status words past the last tile: the failure-injection
+// test waits on it, and nothing ever writes it)
+constexpr size_t NA_STATUS_BYTES = (NA_TILES + 1) * 2 * sizeof(unsigned long long);
 constexpr size_t NA_CTL_OFF = NA_STATUS_OFF + NA_STATUS_BYTES;
 constexpr size_t NA_BYTES = NA_CTL_OFF + 256;
 
@@ -90,7 +100,14 @@ extern "C" {
 
 int s512_partition_i32_noalloc(int* data, size_t left, size_t right, int pivot, size_t* boundary, void* stream) {
     if (!boundary) return S512_ERR_ARG;
-    if (right < left) {
+    int dev = 0;
+    NA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NA_MAX_DEVICES) return S512_ERR_UNSUPPORTED;
+    unsigned char* base = nullptr;
+    int grid = 0;
+    int rc = noalloc_setup(dev, &base, &grid);
+    if (rc) return rc;
+    if (right < left) {  // empty range: the set-up above is all there is to do
         *boundary = left;
         return S512_OK;
     }
@@ -108,13 +125,11 @@ int s512_partition_i32_noalloc(int* data, size_t left, size_t right, int pivot, 
         s512::set_error("s512_partition_i32_noalloc: data must be device memory");
         return S512_ERR_ARG;
     }
-    int dev = 0;
-    NA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= NA_MAX_DEVICES) return S512_ERR_UNSUPPORTED;
-    unsigned char* base = nullptr;
-    int grid = 0;
-    int rc = noalloc_setup(dev, &base, &grid);
-    if (rc) return rc;
+    if (at.type == cudaMemoryTypeDevice && at.device != dev) {
+        s512::set_error("s512_partition_i32_noalloc: data is memory of device %d, the current device is %d",
+                        at.device, dev);
+        return S512_ERR_ARG;
+    }
 
     cudaStream_t st = (cudaStream_t)stream;
     int* keys_out = reinterpret_cast<int*>(base);
@@ -122,21 +137,25 @@ int s512_partition_i32_noalloc(int* data, size_t left, size_t right, int pivot, 
     s512::Part2Ctl* ctl = reinterpret_cast<s512::Part2Ctl*>(base + NA_CTL_OFF);
     const uint32_t ntiles = (uint32_t)((n + NA_TILE - 1) / NA_TILE);
     // the look-back status words and the control block must start at zero
-    NA_TRY(cudaMemsetAsync(status, 0, (size_t)ntiles * 2 * sizeof(unsigned long long), st));
+    NA_TRY(cudaMemsetAsync(status, 0, (size_t)(ntiles + 1) * 2 * sizeof(unsigned long long), st));
     NA_TRY(cudaMemsetAsync(ctl, 0, sizeof(s512::Part2Ctl), st));
     if (grid > (int)ntiles) grid = (int)ntiles;
     s512::partition2_kernel<int, false, NA_THREADS, NA_IPT>
         <<<grid, NA_THREADS, 0, st>>>(data + left, nullptr, keys_out, nullptr, (uint64_t)n, pivot, status, ctl,
-                                      ntiles);
+                                      ntiles, (s512::config().fault_inject & S512_FAULT_TIMEOUT) ? ntiles
+                                                                                                  : 0xFFFFFFFFu);
     NA_TRY(cudaGetLastError());
-    NA_TRY(cudaMemcpyAsync(data + left, keys_out, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
     s512::Part2Ctl h;
     NA_TRY(cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st));
     NA_TRY(cudaStreamSynchronize(st));
     if (h.err) {
+        // tiles that gave up wrote nothing: the scratch holds stale keys, so
+        // the caller's range is left untouched
         s512::set_error("s512_partition_i32_noalloc: look-back wait timed out");
         return S512_ERR_TIMEOUT;
     }
+    NA_TRY(cudaMemcpyAsync(data + left, keys_out, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
+    NA_TRY(cudaStreamSynchronize(st));
     *boundary = left + (size_t)h.total_low;
     return S512_OK;
 }

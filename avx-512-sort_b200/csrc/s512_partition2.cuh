@@ -8,7 +8,7 @@
 // learns how many lows and highs all earlier tiles hold from a decoupled
 // look-back (two counters per tile), and writes lows forward from the start
 // and highs backward from the end of a scratch range, which the host copies
-// back.  The comparison is the reference's own: `x <= pivot` on the caller's
+// back when the kernel reports no error.  The comparison is the reference's own: `x <= pivot` on the caller's
 // type (so a NaN double goes to the high side, as with _CMP_LE_OQ).
 #pragma once
 
@@ -30,7 +30,8 @@ template <typename T, bool KV, int THREADS, int IPT>
 __global__ void __launch_bounds__(THREADS) partition2_kernel(const T* __restrict__ in, const int* __restrict__ vin,
                                                              T* __restrict__ out, int* __restrict__ vout, uint64_t n,
                                                              T pivot, unsigned long long* __restrict__ status,
-                                                             Part2Ctl* ctl, uint32_t ntiles) {
+                                                             Part2Ctl* ctl, uint32_t ntiles,
+                                                             uint32_t inject_slot = 0xFFFFFFFFu) {
     constexpr int NW = THREADS / 32;
     constexpr int TILE = THREADS * IPT;
     constexpr int NC = IPT * NW;  // counters per tile, multiple of 32
@@ -82,6 +83,17 @@ __global__ void __launch_bounds__(THREADS) partition2_kernel(const T* __restrict
             uint64_t prefix = 0;
             if (t == 0) {
                 st_status(st, ST_INC_P2 | mine);
+            } else if (t == 1 && inject_slot != 0xFFFFFFFFu) {
+                // testing: a predecessor that never publishes (the spare
+                // status slot past the last tile), waited for with a short
+                // bound; the tile records the timeout and writes nothing
+                st_status(st, ST_AGG_P2 | mine);
+                uint32_t spins = 0;
+                while (!(ld_status(status + (size_t)inject_slot * 2 + tid) & (ST_INC_P2 | ST_AGG_P2)) &&
+                       ++spins < 1024u)
+                    __nanosleep(100);
+                raise_error(&ctl->err, DEV_ERR_TIMEOUT);
+                prefix = ~0ull;
             } else {
                 st_status(st, ST_AGG_P2 | mine);
                 uint32_t p = t - 1;

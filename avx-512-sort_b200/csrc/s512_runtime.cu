@@ -182,7 +182,18 @@ int pointer_kind(const void* p, int flags) {
         cudaGetLastError();
         return 1;
     }
-    return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) ? 2 : 1;
+    if (at.type == cudaMemoryTypeManaged) return 2;
+    if (at.type != cudaMemoryTypeDevice) return 1;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (at.device != dev) {
+        set_error("pointer %p is memory of device %d, the current device is %d", p, at.device, dev);
+        return 0;
+    }
+    return 2;
 }
 
 }  // namespace s512

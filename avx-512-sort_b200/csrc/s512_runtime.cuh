@@ -94,8 +94,16 @@ class CallGuard {
     std::unique_lock<std::mutex> lk_;
 };
 
-// pointer kind: 1 host, 2 device (or managed)
+// pointer kind: 1 host, 2 device (or managed), 0 memory of a device other
+// than the current one (an error: the kernels run on the current device)
 int pointer_kind(const void* p, int flags);
+
+// `var` = whether p is host memory; returns S512_ERR_ARG from the enclosing
+// function when p belongs to another device
+#define S512_HOST_PTR(var, p, flags)                          \
+    const int var##_kind_ = ::s512::pointer_kind((p), (flags)); \
+    if (var##_kind_ == 0) return S512_ERR_ARG;                \
+    const bool var = var##_kind_ == 1
 
 template <typename F>
 inline cudaError_t launch_persistent(DevCtx& C, F fn, int threads, size_t smem, cudaStream_t st, int max_blocks,

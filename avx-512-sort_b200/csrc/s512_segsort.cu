@@ -192,8 +192,8 @@ static int segsort_entry(int dt, void* keys, void* values, size_t elem_bytes, co
     DevCtx* C = current_ctx(&status);
     if (!C) return status;
     CallGuard guard(C, st);
-    const bool host = pointer_kind(keys, flags) == 1;
-    const bool off_host = pointer_kind(offsets, (flags & S512_PTR_DEVICE) ? 0 : flags) == 1;
+    S512_HOST_PTR(host, keys, flags);
+    S512_HOST_PTR(off_host, offsets, (flags & S512_PTR_DEVICE) ? 0 : flags);
     const size_t* d_off = offsets;
     if (off_host) {
         size_t* o = (size_t*)C->get("seg_offsets", (nseg + 1) * sizeof(size_t));

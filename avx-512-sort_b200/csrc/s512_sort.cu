@@ -30,7 +30,7 @@ int s512_sort_i32(int* data, size_t n, int flags, void* stream) {
     if (!data) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     if (host && stream_needed(n, sizeof(int))) {  // larger than the device budget
         int rc = stream_sort<int>(*C, data, n, st);
         if (rc) return rc;
@@ -53,7 +53,7 @@ int s512_sort_f64(double* data, size_t n, int flags, void* stream) {
     if (!data) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     if (host && stream_needed(n, sizeof(double))) {  // larger than the device budget
         int rc = stream_sort<double>(*C, data, n, st);
         if (rc) return rc;
@@ -76,7 +76,7 @@ int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream) 
     if (!keys || !values) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
-    const bool host = pointer_kind(keys, flags) == 1;
+    S512_HOST_PTR(host, keys, flags);
     int* dk = keys;
     int* dv = values;
     if (host) {
@@ -136,7 +136,7 @@ static int partition_entry(T* data, int* values, size_t left, size_t right, T pi
     const size_t n = right - left + 1;
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     T* dk = data + left;
     int* dv = KV ? values + left : nullptr;
     if (host) {
@@ -158,27 +158,34 @@ static int partition_entry(T* data, int* values, size_t left, size_t right, T pi
     Part2Ctl* ctl = (Part2Ctl*)C->get("p2_ctl", sizeof(Part2Ctl));
     Part2Ctl* hctl = (Part2Ctl*)C->host_pinned(sizeof(Part2Ctl));
     if (!ok || (KV && !ov) || !status || !ctl || !hctl) return S512_ERR_ALLOC;
-    S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)ntiles * 2 * 8, st));
+    // (the spare pair of status words past the last tile is the never-written
+    // predecessor of the failure-injection test)
+    S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(ntiles + 1) * 2 * 8, st));
     S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(Part2Ctl), st));
     auto fn = partition2_kernel<T, KV, THREADS, IPT>;
     int grid = 0;
     S512_CUDA_TRY(launch_persistent(*C, fn, THREADS, 0, st, (int)ntiles, &grid));
-    fn<<<grid, THREADS, 0, st>>>(dk, dv, ok, ov, (uint64_t)n, pivot, status, ctl, ntiles);
+    fn<<<grid, THREADS, 0, st>>>(dk, dv, ok, ov, (uint64_t)n, pivot, status, ctl, ntiles,
+                                 (config().fault_inject & S512_FAULT_TIMEOUT) ? ntiles : 0xFFFFFFFFu);
     S512_LAUNCH_CHECK();
+    // the error word first: tiles that gave up wrote nothing, so on an error
+    // the scratch holds stale keys and the caller's range stays as it was
+    S512_CUDA_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(Part2Ctl), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hctl->err) {
+        guard_.finish();
+        set_error("partition look-back wait timed out");
+        return S512_ERR_TIMEOUT;
+    }
     T* dst = host ? dk : data + left;
     S512_CUDA_TRY(cudaMemcpyAsync(dst, ok, n * sizeof(T), cudaMemcpyDeviceToDevice, st));
     if (KV) S512_CUDA_TRY(cudaMemcpyAsync(host ? dv : values + left, ov, n * sizeof(int), cudaMemcpyDeviceToDevice, st));
-    S512_CUDA_TRY(cudaMemcpyAsync(hctl, ctl, sizeof(Part2Ctl), cudaMemcpyDeviceToHost, st));
     if (host) {
         S512_CUDA_TRY(cudaMemcpyAsync(data + left, dk, n * sizeof(T), cudaMemcpyDeviceToHost, st));
         if (KV) S512_CUDA_TRY(cudaMemcpyAsync(values + left, dv, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     guard_.finish();
     S512_CUDA_TRY(cudaStreamSynchronize(st));
-    if (hctl->err) {
-        set_error("partition look-back wait timed out");
-        return S512_ERR_TIMEOUT;
-    }
     s512_stats& S = thread_stats();
     memset(&S, 0, sizeof(S));
     S.kernel_launches = 1;

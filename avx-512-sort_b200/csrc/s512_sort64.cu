@@ -21,7 +21,7 @@ static int sort_words(T* data, size_t n, int flags, void* stream) {
     DevCtx* C = current_ctx(&status);
     if (!C) return status;
     CallGuard guard(C, st);
-    const bool host = pointer_kind(data, flags) == 1;
+    S512_HOST_PTR(host, data, flags);
     if constexpr (std::is_same<Codec, CodecI64>::value) {
         if (host && stream_needed(n, 8)) {  // larger than the device budget
             int rc = stream_sort<long long>(*C, data, n, st);

@@ -36,6 +36,19 @@ def _default_merge(t, middle: int):
     sort512cuda.merge(t, middle)
 
 
+def order_keys(t):
+    """Integers whose order is the library's sort order of `t`: the values
+    themselves for integer tensors; for float64 the IEEE total order (-NaN
+    first, then -inf .. -0.0, +0.0 .. +inf, +NaN last), as int64 whose signed
+    order matches it.  The cut points are searched in these keys, since IEEE
+    compares do not order NaNs and tie -0.0 with +0.0."""
+    import torch
+    if t.dtype != torch.float64:
+        return t
+    b = t.view(torch.int64)
+    return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFF)
+
+
 def splitters_from_samples(samples, nranks: int):
     """P-1 splitters at the quantiles of the sorted, gathered sample."""
     m = samples.numel()
@@ -108,9 +121,10 @@ def sort_sharded(x, group=None, oversample: int = 256, local_sort: Optional[Call
     local_sort(allsamp)
     spl = splitters_from_samples(allsamp, P)
 
-    # 4. cut points: keys <= splitter r go to ranks <= r
+    # 4. cut points: keys <= splitter r (in the sort's order) go to ranks <= r
     if spl.numel():
-        cuts = torch.searchsorted(x, spl, right=True).to(torch.int64)
+        cuts = torch.searchsorted(order_keys(x).contiguous(), order_keys(spl).contiguous(),
+                                  right=True).to(torch.int64)
     else:
         cuts = torch.zeros(P - 1, dtype=torch.int64, device=x.device)
     edges = torch.cat([torch.zeros(1, dtype=torch.int64, device=x.device), cuts,

@@ -235,9 +235,25 @@ def core_small_sort(a, nvec: int, flags: int = 0, stream=None) -> None:
     _check(fn, getattr(lib(), fn)(p, nvec, _flags(dev, flags), _stream(stream)))
 
 
+def _check_range(left: int, right: int, n: int) -> bool:
+    """Validate an inclusive range [left, right] of an n-element array before
+    it reaches the C ABI (which takes size_t and trusts it).  Returns False
+    for an empty range (right < left), which needs no call."""
+    left, right = int(left), int(right)
+    if right < left:
+        if left < 0 or left > n:
+            raise ValueError(f"empty range starts at {left}, outside 0..{n}")
+        return False
+    if left < 0 or right >= n:
+        raise ValueError(f"range [{left}, {right}] is outside the array's {n} elements")
+    return True
+
+
 def partition(a, left: int, right: int, pivot, flags: int = 0, stream=None) -> int:
     """Sort512::Partition512: returns the first index whose value is > pivot."""
     p, n, dt, dev = _ptr(a)
+    if not _check_range(left, right, n):
+        return int(left)
     out = ctypes.c_size_t(0)
     fn = f"s512_partition_{_suffix(dt)}"
     _check(fn, getattr(lib(), fn)(p, left, right, pivot, ctypes.byref(out), _flags(dev, flags), _stream(stream)))
@@ -342,8 +358,10 @@ def core_small_sort_kv(keys, values, nvec: int, flags: int = 0, stream=None) -> 
 
 
 def partition_kv(keys, values, left: int, right: int, pivot: int, flags: int = 0, stream=None) -> int:
-    pk, _, _, dev = _ptr(keys)
-    pv, _, _, _ = _ptr(values)
+    pk, n, _, dev = _ptr(keys)
+    pv, nv, _, _ = _ptr(values)
+    if not _check_range(left, right, min(n, nv)):
+        return int(left)
     out = ctypes.c_size_t(0)
     _check("s512_partition_kv_i32", lib().s512_partition_kv_i32(pk, pv, left, right, pivot, ctypes.byref(out),
                                                                 _flags(dev, flags), _stream(stream)))
@@ -356,6 +374,8 @@ def partition_noalloc(a, left: int, right: int, pivot: int, stream=None) -> int:
     p, n, dt, dev = _ptr(a)
     if dt != "int32" or not dev:
         raise ValueError("partition_noalloc takes an int32 CUDA tensor")
+    if not _check_range(left, right, n):
+        return int(left)
     out = ctypes.c_size_t(0)
     _check("s512_partition_i32_noalloc",
            lib().s512_partition_i32_noalloc(p, left, right, pivot, ctypes.byref(out), _stream(stream)))

@@ -34,6 +34,7 @@ PART_DRAM_BYTES_PER_KEY = 16.03
 PKG = os.path.join(ROOT, "avx-512-sort_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
 
 METRIC = "Gkeys/s at 2^28 int32/f64/kv; learned vs plain splitters; % of HBM roofline"
 N_KEYS = 1 << 28
@@ -152,58 +153,150 @@ def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_sort(n: int, threads: int, fn: str = "sort_omp_partition", dtype="f64", seed=1):
-    """Time the reference (compiled in place) or, without AVX-512, the C
-    restatement, on `n` keys of the workload.  Returns (seconds, kind, cores)."""
+# The reference's CPU path (compiled in place from its sources by oracle/Makefile)
+def cpu_reference():
+    """(checker, kind): the reference compiled in place when this host has
+    AVX-512, else the C restatement (single-threaded `Sort` only)."""
     sys.path.insert(0, ORACLE_DIR)
-    import numpy as np
-
-    import workloads
     from oracle import REF_SO, Oracle, Reference, cpu_has_avx512
-    a = workloads.uniform01_np(n, seed) if dtype == "f64" else workloads.uniform_i32_np(n, seed)
     if os.path.exists(REF_SO) and cpu_has_avx512():
-        ref = Reference()
-        ref.set_threads(threads)
-        t0 = time.perf_counter()
-        ref.call(fn, a)
-        dt = time.perf_counter() - t0
-        kind, cores = "reference", (threads if fn != "sort" else 1)
-    else:
-        o = Oracle()
-        t0 = time.perf_counter()
-        o.sort(a)
-        dt = time.perf_counter() - t0
-        kind, cores = "port", 1
-    assert bool(np.all(a[1:] >= a[:-1]))
-    return dt, kind, cores
+        return Reference(), "reference"
+    return Oracle(), "port"
+
+
+REF_FUNCTIONS = {"sort_omp_partition": "Sort512::SortOmpPartition", "sort": "Sort512::Sort",
+                 "kv_sort_omp_partition": "Sort512kv::SortOmpPartition"}
+
+
+def time_reference(ref, kind, fn, base, threads, reps, vals=None, keep=None):
+    """Seconds of each of `reps` runs of reference function `fn` on a fresh
+    copy of `base` (copied outside the timed region); the last output is
+    checked for sortedness (and left in `keep`, a list, when one is given).
+    kv functions take `vals` too."""
+    import numpy as np
+    work = np.empty_like(base)
+    vwork = np.empty_like(vals) if vals is not None else None
+    times = []
+    for _ in range(reps):
+        np.copyto(work, base)
+        if vwork is not None:
+            np.copyto(vwork, vals)
+        if kind == "reference":
+            ref.set_threads(threads)
+            t0 = time.perf_counter()
+            if fn.startswith("kv_"):
+                ref.call_kv(fn[3:], work, vwork)
+            else:
+                ref.call(fn, work)
+        else:  # the restatement: one core, Sort
+            t0 = time.perf_counter()
+            if fn.startswith("kv_"):
+                ref.sort_kv(work, vwork)
+            else:
+                ref.sort(work)
+        times.append(time.perf_counter() - t0)
+    if work.size > 1:
+        assert bool(np.all(work[1:] >= work[:-1])), f"reference {fn} output not sorted"
+    if keep is not None:
+        keep.append(work)
+    return times
+
+
+def _median(v):
+    v = sorted(v)
+    return v[len(v) // 2]
 
 
 def run_reference_arm(args, world, rank):
-    """--impl reference: the reference's own CPU sort on this host's cores."""
+    """--impl reference: the reference's own CPU sort (SortOmpPartition on all
+    host cores) on the full workload, one sort per step, the input restored
+    from an untimed copy before each step."""
     if rank != 0:
         return
+    import numpy as np
+
+    import workloads
     threads = os.cpu_count() or 1
-    n = min(args.n, 1 << 26)  # bounded sample of the 2^28 workload per step
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_reference_sort(1 << 20, threads)
-    times = []
-    kind, cores = "port", 1
-    for s in range(args.steps):
-        dt, kind, cores = cpu_reference_sort(n, threads, seed=100 + s)
-        times.append(dt)
+    n = args.n
+    base = workloads.uniform01_np(n, 1)
+    ref, kind = cpu_reference()
+    cores = threads if kind == "reference" else 1
+    if args.warmup:
+        time_reference(ref, kind, "sort_omp_partition", base, threads, args.warmup)
+    times = time_reference(ref, kind, "sort_omp_partition", base, threads, args.steps)
     tot = sum(times)
     val = n * len(times) / tot / 1e9
+    fname = REF_FUNCTIONS["sort_omp_partition"] if kind == "reference" else "restated CoreSort (1 core)"
     line = {
         "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "Gkeys/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(tot / len(times) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": args.n, "sample_n_per_step": n,
-                   "function": "Sort512::SortOmpPartition" if kind == "reference" else "restated CoreSort"},
+        "config": {"workload": WORKLOAD, "n": n, "function": fname,
+                   "median_ms_per_step": round(_median(times) * 1e3, 3)},
         "cpu_baseline": {"value": round(val, 4), "unit": "Gkeys/s", "cores": cores, "kind": kind,
-                         "sample": f"{n} uniform doubles per step, {args.steps} steps"},
+                         "sample": f"the full workload: {n} uniform doubles per step, {args.steps} steps "
+                                   f"({fname}, {cores} threads)"},
         "e2e": {"value": round(val, 4), "unit": "Gkeys/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_rows(n, dev):
+    """The reference on this host's cores, same inputs as the GPU rows:
+    SortOmpPartition (all cores, median of 5) and Sort (1 core) on the
+    headline 2^28 doubles, the kv SortOmpPartition on 2^28 pairs, the normal
+    distribution at 2^28, and the three distributions on which the
+    reference's pivot rule is quadratic (ascending, descending, 256 distinct
+    values) at the largest size that finishes under a per-run cap.  Returns
+    (headline entry, rows)."""
+    import numpy as np
+
+    import workloads
+    threads = os.cpu_count() or 1
+    ref, kind = cpu_reference()
+    cores = threads if kind == "reference" else 1
+    rows = {}
+    base = workloads.uniform01_torch(n, seed=1, device=dev).cpu().numpy()
+    t = time_reference(ref, kind, "sort_omp_partition", base, threads, 5)
+    head = {"value": round(n / _median(t) / 1e9, 4), "unit": "Gkeys/s", "cores": cores, "kind": kind,
+            "sample": (f"{REF_FUNCTIONS['sort_omp_partition']} on the full workload ({n} uniform doubles), "
+                       f"median of 5 runs, {threads} threads") if kind == "reference"
+            else f"restated CoreSort on {n} uniform doubles, 1 core, median of 5 runs",
+            "runs_ms": [round(x * 1e3, 1) for x in t]}
+    if kind != "reference":
+        return head, rows
+    t = time_reference(ref, kind, "sort", base, 1, 1)
+    rows["f64_uniform_sort_1core"] = {"n": n, "ms": round(t[0] * 1e3, 1), "gkeys_s": round(n / t[0] / 1e9, 4),
+                                      "function": REF_FUNCTIONS["sort"], "cores": 1}
+    del base
+    x = workloads.double_dist_torch("normal", n, seed=2, device=dev).cpu().numpy()
+    t = time_reference(ref, kind, "sort_omp_partition", x, threads, 3)
+    rows["f64_normal"] = {"n": n, "ms_median": round(_median(t) * 1e3, 1),
+                          "gkeys_s": round(n / _median(t) / 1e9, 4), "cores": threads}
+    del x
+    k = workloads.uniform_i32_torch(n, 9, dev).cpu().numpy()
+    v = np.arange(n, dtype=np.int32)
+    t = time_reference(ref, kind, "kv_sort_omp_partition", k, threads, 3, vals=v)
+    rows["kv_uniform"] = {"n": n, "ms_median": round(_median(t) * 1e3, 1), "gkeys_s": round(n / _median(t) / 1e9, 4),
+                          "function": REF_FUNCTIONS["kv_sort_omp_partition"], "cores": threads}
+    del k, v
+    cap_s = 4.0
+    for dist in ("ascending", "descending", "distinct256"):
+        m, done = 1 << 16, None
+        while m <= n:
+            x = workloads.double_dist_torch(dist, m, seed=3, device=dev).cpu().numpy()
+            out = []
+            t = time_reference(ref, kind, "sort_omp_partition", x, threads, 1, keep=out)[0]
+            done = {"n": m, "ms": round(t * 1e3, 1), "gkeys_s": round(m / t / 1e9, 5),
+                    "equal_to_np_sort": bool(np.array_equal(out[0], np.sort(x)))}
+            if 4 * t > cap_s:  # the next size (quadratic) would pass the cap
+                break
+            m *= 2
+        rows[f"f64_{dist}"] = dict(done, cap_s_per_run=cap_s,
+                                   note=("finished at the full size" if done["n"] >= n else
+                                         f"did not run at 2^{n.bit_length() - 1}: the next doubling "
+                                         f"would exceed {cap_s} s (quadratic in the reference)"))
+    return head, rows
 
 
 # ---------------------------------------------------------------------------
@@ -228,10 +321,13 @@ def run_ours(args, world, rank, local):
         x = make(900 + w)
         s512.sort(x, flags=s512.ASYNC, stream=stream)
         torch.cuda.synchronize()
-        assert bool((x[1:] >= x[:-1]).all()), "warm-up output not sorted"
+        assert workloads.is_sorted_torch(x), "warm-up output not sorted"
         del x
-    # distinct inputs for every timed step, generated before timing
+    # distinct inputs for every timed step, generated before timing, with the
+    # multiset fingerprint of each and a copy of the first (checked in full)
     inputs = [make(s) for s in range(args.steps)]
+    fps = [workloads.multiset_fingerprint_torch(x) for x in inputs]
+    first = inputs[0].clone()
     torch.cuda.synchronize()
     barrier(world)
 
@@ -261,8 +357,15 @@ def run_ours(args, world, rank, local):
     clocks = sampler.stop() if sampler else None
     dev_ms = ev0.elapsed_time(ev1)
     dev_ms = max_over_ranks(dev_ms, world)
-    ok = all(bool((x[1:] >= x[:-1]).all()) for x in inputs)
-    del inputs
+    # every step: sorted, and the same multiset as its input; the first step
+    # also equal, key for key, to an independent sort of its input
+    verify = {"sorted_every_step": all(workloads.is_sorted_torch(x) for x in inputs),
+              "multiset_every_step": all(workloads.multiset_fingerprint_torch(x) == f
+                                         for x, f in zip(inputs, fps)),
+              "first_step_equal_to_torch_sort": bool(torch.equal(
+                  workloads.order_keys_torch(inputs[0]), torch.sort(workloads.order_keys_torch(first)).values))}
+    ok = all(verify.values())
+    del inputs, first
     torch.cuda.empty_cache()
     ms_per_step = dev_ms / args.steps
     value = n * world / (ms_per_step * 1e-3) / 1e9
@@ -322,16 +425,13 @@ def run_ours(args, world, rank, local):
     except Exception as e:  # noqa: BLE001
         e2e = {"value": None, "unit": "Gkeys/s", "error": str(e)[:200]}
 
-    # CPU baseline: the reference's SortOmpPartition on all host cores
+    # CPU baseline: the reference's SortOmpPartition on all host cores, on
+    # the full workload, with the reference's other rows beside it
     cpu = None
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:
         try:
-            threads = os.cpu_count() or 1
-            sn = 1 << 26
-            dt, kind, cores = cpu_reference_sort(sn, threads)
-            cpu = {"value": round(sn / dt / 1e9, 4), "unit": "Gkeys/s", "cores": cores, "kind": kind,
-                   "sample": f"Sort512::SortOmpPartition on {sn} uniform doubles (one run)" if kind == "reference"
-                   else f"restated CoreSort on {sn} uniform doubles, 1 core"}
+            cpu, rows = cpu_baseline_rows(n, dev)
+            cpu["rows"] = rows
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "Gkeys/s", "error": str(e)[:200]}
 
@@ -347,7 +447,7 @@ def run_ours(args, world, rank, local):
                    "l2": "inputs larger than L2: a distinct 2 GiB input per step",
                    "levels": levels},
         "clocks": clocks, "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-        "gpu_launches": launches, "sorted_ok": ok, "stats_last_step": last, "extras": extras,
+        "gpu_launches": launches, "sorted_ok": ok, "verify": verify, "stats_last_step": last, "extras": extras,
     }
     print(json.dumps(line), flush=True)
 
@@ -415,39 +515,68 @@ def _timed(fn, stream):
     return e0.elapsed_time(e1)
 
 
+EXTRA_REPS = 10
+
+
+def _median_timed(run, restore, stream, reps=EXTRA_REPS, warm=2):
+    """Median device time (ms) of `reps` timed runs, each on a fresh input
+    (restore() copies it back, untimed), after `warm` untimed runs."""
+    import torch
+    for _ in range(warm):
+        restore()
+        run()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        restore()
+        times.append(_timed(run, stream))
+    return _median(times), times
+
+
 def run_extras(n, dev, stream):
-    """One timed run per extra workload (reported beside the headline)."""
+    """The other workloads at full size, each the median of EXTRA_REPS timed
+    runs on a restored input, each output checked: sorted and the same
+    multiset as its input (key/value: the same (key, value) pairs)."""
     import torch
 
     import sort512cuda as s512
     import workloads
     out = {}
 
+    def verified(x, fp, *more):
+        return workloads.is_sorted_torch(x) and workloads.multiset_fingerprint_torch(x, *more) == fp
+
     for dist in workloads.DOUBLE_DISTS:
-        x = workloads.double_dist_torch(dist, n, seed=5, device=dev)
-        s512.sort(x, flags=s512.ASYNC, stream=stream)  # warm
-        x = workloads.double_dist_torch(dist, n, seed=6, device=dev)
-        ms = _timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream)
-        ok = bool((x[1:] >= x[:-1]).all())
+        x0 = workloads.double_dist_torch(dist, n, seed=6, device=dev)
+        fp = workloads.multiset_fingerprint_torch(x0)
+        x = torch.empty_like(x0)
+        ms, _ = _median_timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), lambda: x.copy_(x0), stream)
         st = s512.stats()
-        out[f"f64_{dist}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "sorted": ok,
-                              "levels": st["levels"], "fallbacks": st["fallbacks"]}
-        del x
-    x = workloads.uniform_i32_torch(n, seed=8, device=dev)
-    s512.sort(x.clone(), flags=s512.ASYNC, stream=stream)
-    ms = _timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream)
-    out["i32_uniform"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
-                          "sorted": bool((x[1:] >= x[:-1]).all())}
-    del x
+        out[f"f64_{dist}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "verified": verified(x, fp),
+                              "levels": st["levels"], "fallbacks": st["fallbacks"], "reps": EXTRA_REPS}
+        del x, x0
+    x0 = workloads.uniform_i32_torch(n, seed=8, device=dev)
+    fp = workloads.multiset_fingerprint_torch(x0)
+    x = torch.empty_like(x0)
+    ms, _ = _median_timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), lambda: x.copy_(x0), stream)
+    out["i32_uniform"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "verified": verified(x, fp),
+                          "reps": EXTRA_REPS}
+    del x, x0
     for kname in ("uniform", "zipf"):
-        k = workloads.uniform_i32_torch(n, 9, dev) if kname == "uniform" else workloads.zipf_i32_torch(n, seed=9,
-                                                                                                         device=dev)
-        v = torch.arange(n, dtype=torch.int32, device=dev)
-        s512.sort_kv(k.clone(), v.clone(), flags=s512.ASYNC, stream=stream)
-        ms = _timed(lambda: s512.sort_kv(k, v, flags=s512.ASYNC, stream=stream), stream)
-        out[f"kv_{kname}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
-                              "sorted": bool((k[1:] >= k[:-1]).all())}
-        del k, v
+        k0 = workloads.uniform_i32_torch(n, 9, dev) if kname == "uniform" else workloads.zipf_i32_torch(n, seed=9,
+                                                                                                          device=dev)
+        v0 = torch.arange(n, dtype=torch.int32, device=dev)
+        fp = workloads.multiset_fingerprint_torch(k0, v0)
+        k, v = torch.empty_like(k0), torch.empty_like(v0)
+
+        def restore():
+            k.copy_(k0)
+            v.copy_(v0)
+
+        ms, _ = _median_timed(lambda: s512.sort_kv(k, v, flags=s512.ASYNC, stream=stream), restore, stream)
+        out[f"kv_{kname}"] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3), "verified": verified(k, fp, v),
+                              "reps": EXTRA_REPS}
+        del k, v, k0, v0
     torch.cuda.empty_cache()
     out["int32_2p20_latency"] = extra_c1(dev, stream)
     out["learned_vs_plain"] = extra_learned(dev, stream)
@@ -476,38 +605,25 @@ def extra_c1(dev, stream):
         torch.cuda.synchronize()
         times.append(_timed(lambda: s512.sort(x, flags=s512.ASYNC, stream=stream), stream))
     dev_ms = float(np.median(times[3:]))
-    h = a.copy()
-    t0 = time.perf_counter()
-    s512.sort(h)
-    host_ms = (time.perf_counter() - t0) * 1e3
+    host_times = []
+    for _ in range(7):  # host pointer (pageable numpy memory): copy in, sort, copy out
+        h = a.copy()
+        t0 = time.perf_counter()
+        s512.sort(h)
+        host_times.append((time.perf_counter() - t0) * 1e3)
+    host_ms = _median(host_times[2:])
     with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
         want = json.load(f)["c1"]["sorted"]
     exact = hashlib.sha256(h.tobytes()).hexdigest()[:32] == want
     cpu_ms = None
     try:
-        b = a.copy()
-        dt, kind, _ = cpu_reference_sort_array(b, "sort")
-        cpu_ms = dt * 1e3
+        ref, kind = cpu_reference()
+        cpu_ms = _median(time_reference(ref, kind, "sort", a, 1, 5)) * 1e3
     except Exception:  # noqa: BLE001
         kind = "unavailable"
     return {"n": n, "device_ms_median": round(dev_ms, 4), "gkeys_s": round(n / dev_ms / 1e6, 3),
             "host_pointer_call_ms": round(host_ms, 3), "exact_vs_reference_digest": exact,
-            "reference_sort_1core_ms": round(cpu_ms, 3) if cpu_ms else None, "reference_kind": kind}
-
-
-def cpu_reference_sort_array(a, fn="sort", threads=1):
-    sys.path.insert(0, ORACLE_DIR)
-    from oracle import REF_SO, Oracle, Reference, cpu_has_avx512
-    if os.path.exists(REF_SO) and cpu_has_avx512():
-        ref = Reference()
-        ref.set_threads(threads)
-        t0 = time.perf_counter()
-        ref.call(fn, a)
-        return time.perf_counter() - t0, "reference", threads
-    o = Oracle()
-    t0 = time.perf_counter()
-    o.sort(a)
-    return time.perf_counter() - t0, "port", 1
+            "reference_sort_1core_ms_median": round(cpu_ms, 3) if cpu_ms else None, "reference_kind": kind}
 
 
 def extra_learned(dev, stream):
@@ -527,6 +643,7 @@ def extra_learned(dev, stream):
     for name, make in cases:
         x0 = make()
         n = x0.numel()
+        fp = workloads.multiset_fingerprint_torch(x0)
         row = {"n": n}
         for mode, flag in (("plain", s512.SPLIT_PLAIN), ("learned", s512.SPLIT_LEARNED)):
             x = x0.clone()
@@ -534,10 +651,10 @@ def extra_learned(dev, stream):
                 x.copy_(x0)
                 s512.sort(x, flags=flag | s512.ASYNC, stream=stream)
             times = []
-            for _ in range(3):
+            for _ in range(EXTRA_REPS):
                 x.copy_(x0)
                 times.append(_timed(lambda: s512.sort(x, flags=flag | s512.ASYNC, stream=stream), stream))
-            ms = sorted(times)[1]
+            ms = _median(times)
             st = s512.stats()
             row[mode] = {"gkeys_s": round(n / ms / 1e6, 3), "ms": round(ms, 3),
                          "partition_ms": round(sum(st["partition_ms"]), 3),
@@ -546,7 +663,8 @@ def extra_learned(dev, stream):
                          "models_rejected": st["learned_rejected"], "fallbacks": st["fallbacks"],
                          "max_bucket_over_mean": [round(v, 2) for v in st["max_bucket_over_mean"]],
                          "bucket_cv": [round(v, 3) for v in st["bucket_cv"]],
-                         "sorted": bool((x[1:] >= x[:-1]).all())}
+                         "verified": workloads.is_sorted_torch(x) and
+                         workloads.multiset_fingerprint_torch(x) == fp, "reps": EXTRA_REPS}
             del x
         rows[name] = row
         del x0
@@ -570,6 +688,7 @@ def extra_segsort(dev, stream):
     off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
     total = int(off[-1])
     d_off = torch.from_numpy(off.view(np.int64)).to(dev)
+    seg_id = torch.repeat_interleave(torch.arange(nseg, device=dev), torch.from_numpy(lens).to(dev))
     res = {"segments": nseg, "keys": total}
     tuned = {}
     for dt in (s512.DTYPE_I32, s512.DTYPE_F64, s512.DTYPE_KV_I32):
@@ -583,14 +702,25 @@ def extra_segsort(dev, stream):
         keys = keys0.clone()
         vals = vals0.clone() if vals0 is not None else None
         plan = s512.SegsortPlan(dt, keys, d_off, values=vals)
-        times = []
-        for rep in range(4):
+        def restore():
             keys.copy_(keys0)
             if vals is not None:
                 vals.copy_(vals0)
-            times.append(_timed(lambda: plan.launch(stream), stream))
+
+        ms, _ = _median_timed(lambda: plan.launch(stream), restore, stream)
         plan.close()
-        ms = float(np.median(times[1:]))
+        # every segment: equal to a segment-wise sort of its input (two
+        # stable torch sorts: by key, then by segment)
+        if dt == s512.DTYPE_KV_I32:
+            key0 = keys0.to(torch.int64) * (1 << 32) + (vals0.to(torch.int64) + (1 << 31))
+            got = keys.to(torch.int64) * (1 << 32) + (vals.to(torch.int64) + (1 << 31))
+        else:
+            key0 = workloads.order_keys_torch(keys0)
+            got = workloads.order_keys_torch(keys)
+        p1 = torch.sort(key0, stable=True).indices
+        p2 = torch.sort(seg_id[p1], stable=True).indices
+        every_segment_ok = bool(torch.equal(got, key0[p1[p2]]))
+        del key0, got, p1, p2
         # a loop of single-array sorts over every 100th segment, scaled up
         idx = list(range(0, nseg, 100))
         sub = keys0.clone()
@@ -602,13 +732,9 @@ def extra_segsort(dev, stream):
                                   for i in idx], stream)
         sample_keys = int(sum(int(off[i + 1] - off[i]) for i in idx))
         loop_est_ms = loop_ms * total / max(sample_keys, 1)
-        ok = True
-        kh = keys.cpu().numpy()
-        for i in idx[::20]:
-            seg = kh[int(off[i]):int(off[i + 1])]
-            ok = ok and bool(np.all(seg[1:] >= seg[:-1]))
         row = {"gkeys_s": round(total / ms / 1e6, 3), "ms": round(ms, 3), "launch_shape": tuned[dt],
-               "loop_of_sorts_est_ms": round(loop_est_ms, 1), "sorted_sample": ok}
+               "loop_of_sorts_est_ms": round(loop_est_ms, 1), "every_segment_verified": every_segment_ok,
+               "reps": EXTRA_REPS}
         # the reference's loop on the host for the same sample of segments
         try:
             sys.path.insert(0, ORACLE_DIR)

@@ -239,9 +239,15 @@ S512_API int s512_popcount(unsigned mask);
  *     same kernel and result as s512_partition_i32 with S512_PTR_DEVICE, but
  *     its scratch is a fixed device array of S512_NOALLOC_MAX_ELEMS ints plus
  *     a few KB, held by every GPU that loads the library until exit.  Larger
- *     ranges return S512_ERR_ARG.  The first call on a device looks up that
- *     array and should come before any stream capture; calls that overlap on
- *     the GPU share the array and race.  Waits for the result. */
+ *     ranges return S512_ERR_ARG, and so does data that is not memory of the
+ *     current device (managed memory is accepted).  The first call on a
+ *     device does the set-up: it looks up that array, and since CUDA loads
+ *     modules lazily by default, the driver reserves the array's memory then.
+ *     Make that first call at start-up, before another allocator owns the
+ *     device's memory and before any stream capture; a call with an empty
+ *     range (right < left) does only the set-up.  Calls that overlap on the
+ *     GPU share the array and race.  Waits for the result; on an error the
+ *     caller's data is left as it was. */
 #define S512_NOALLOC_MAX_ELEMS (1u << 20)
 S512_API int s512_partition_i32_noalloc(int* data, size_t left, size_t right, int pivot, size_t* boundary,
                                         void* stream);

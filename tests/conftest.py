@@ -7,7 +7,7 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "avx-512-sort_b200")
 ORACLE_DIR = os.path.join(ROOT, "oracle")
-for p in (PKG, ORACLE_DIR):
+for p in (ROOT, PKG, ORACLE_DIR):
     if p not in sys.path:
         sys.path.insert(0, p)
 

@@ -1,7 +1,7 @@
 """Generate tests/golden/golden.json from the reference compiled in place.
 
-Run in a container that has the reference sources (REFDIR, default
-/root/reference) and an AVX-512 CPU:
+Run where the reference sources are (oracle/Makefile's REFDIR) on an
+AVX-512 CPU:
 
     make -C oracle all && python tests/golden/make_golden.py
 
@@ -23,7 +23,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
-sys.path.insert(0, os.path.join(ROOT, "avx-512-sort_b200"))
+sys.path.insert(0, ROOT)
 
 from oracle import Oracle, Reference  # noqa: E402
 import workloads  # noqa: E402

@@ -92,3 +92,19 @@ def test_no_device_fails_loudly(s512):
     assert rc == s512.S512_ERR_UNSUPPORTED
     assert s512.lib().s512_last_error_string()
     assert np.array_equal(a, np.arange(100, dtype=np.int32)[::-1])
+
+
+def test_partition_ranges_are_checked_before_the_call(s512):
+    # an index past the array (or a negative one, which size_t would wrap)
+    # is refused in Python and never reaches the library, so no device work
+    # starts; an empty range returns `left` without a call
+    import numpy as np
+    import pytest
+    a = np.arange(10, dtype=np.int32)
+    for left, right in ((0, 10), (-1, 5), (3, 12), (11, 20)):
+        with pytest.raises(ValueError):
+            s512.partition(a, left, right, 4)
+    with pytest.raises(ValueError):
+        s512.partition_kv(a, a[:5].copy(), 0, 7, 4)
+    assert s512.partition(a, 5, 4, 0) == 5
+    assert s512.partition(a, 0, -1, 0) == 0

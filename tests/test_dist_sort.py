@@ -25,7 +25,25 @@ def _shard(rank, case):
         return rng.integers(-2 ** 31, 2 ** 31 - 1, 5000 + 1000 * rank).astype(np.int32)
     if case == 1:  # many repeats, one empty shard
         return np.zeros(0, np.int32) if rank == 1 else rng.integers(0, 7, 3000).astype(np.int32)
-    return rng.standard_normal(4000 - 500 * rank)  # float64
+    if case == 2:
+        return rng.standard_normal(4000 - 500 * rank)  # float64
+    # float64 with signed zeros, infinities and NaNs of both signs
+    x = rng.standard_normal(3000 + 300 * rank)
+    special = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, -np.nan] * (40 + 10 * rank))
+    x[rng.choice(x.size, special.size, replace=False)] = special
+    return x
+
+
+def _total_order_key(a):
+    """int64 keys whose signed order is the IEEE total order of float64."""
+    b = np.ascontiguousarray(a, dtype=np.float64).view(np.int64)
+    return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFF)
+
+
+def _sort_like_library(a):
+    if a.dtype != np.float64:
+        return np.sort(a)
+    return a[np.argsort(_total_order_key(a), kind="stable")]
 
 
 def _rank_main(rank, world, port, case, out):
@@ -36,11 +54,16 @@ def _rank_main(rank, world, port, case, out):
     sys.path.insert(0, os.path.join(ROOT, "avx-512-sort_b200"))
     import dist_sort
 
+    # the library's order: IEEE total order for doubles (-0.0 before +0.0,
+    # NaNs at the ends by sign)
     def cpu_sort(t):
-        t.copy_(torch.sort(t).values)
+        if t.dtype == torch.float64:
+            t.copy_(t[torch.argsort(dist_sort.order_keys(t), stable=True)])
+        else:
+            t.copy_(torch.sort(t).values)
 
     def cpu_merge(t, middle):
-        t.copy_(torch.sort(t).values)
+        cpu_sort(t)
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
@@ -52,7 +75,7 @@ def _rank_main(rank, world, port, case, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,case", [(2, 0), (3, 1), (3, 2)])
+@pytest.mark.parametrize("world,case", [(2, 0), (3, 1), (3, 2), (2, 3), (3, 3)])
 def test_sharded_sort_is_the_sorted_union(world, case):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
@@ -65,12 +88,16 @@ def test_sharded_sort_is_the_sorted_union(world, case):
     for p in procs:
         p.join(timeout=120)
         assert p.exitcode == 0
-    union = np.sort(np.concatenate([_shard(r, case) for r in range(world)]))
+    union = _sort_like_library(np.concatenate([_shard(r, case) for r in range(world)]))
     joined = np.concatenate([got[r] for r in range(world)])
-    assert np.array_equal(joined, union)
-    for r in range(world - 1):  # range partitioned
+    # bit-exact (NaN payloads and signed zeros included)
+    assert joined.dtype == union.dtype and np.array_equal(joined.view(np.uint8), union.view(np.uint8))
+    for r in range(world - 1):  # range partitioned, in the library's order
         if got[r].size and got[r + 1].size:
-            assert got[r][-1] <= got[r + 1][0]
+            if union.dtype == np.float64:
+                assert _total_order_key(got[r][-1:])[0] <= _total_order_key(got[r + 1][:1])[0]
+            else:
+                assert got[r][-1] <= got[r + 1][0]
 
 
 def test_merge_runs_pairs_neighbours():

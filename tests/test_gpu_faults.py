@@ -71,3 +71,45 @@ def test_lookback_timeout_is_reported_and_device_stays_usable(faults, cuda):
     t = t0.clone()
     s512.sort(t)
     assert torch.equal(t, torch.sort(t0).values)
+
+
+def test_partition_timeout_leaves_the_data_untouched(faults, cuda):
+    # Partition512 writes into scratch and copies back only after the kernel
+    # reported no error: after an injected look-back timeout the caller's
+    # range (device or host memory, keys and values) is as it was
+    import numpy as np
+    import torch
+    import workloads
+    s512 = faults
+    n = 1 << 20
+    k0 = workloads.uniform_i32_torch(n, 6)
+    v0 = torch.arange(n, dtype=torch.int32, device=cuda)
+    s512.set_config(fault_inject=s512.FAULT_TIMEOUT)
+    try:
+        k = k0.clone()
+        with pytest.raises(s512.Sort512Error) as e:
+            s512.partition(k, 0, n - 1, 0)
+        assert e.value.code == s512.S512_ERR_TIMEOUT
+        assert torch.equal(k, k0)
+        hk = k0.cpu().numpy().copy()
+        with pytest.raises(s512.Sort512Error) as e:
+            s512.partition(hk, 10, n - 11, 0)
+        assert e.value.code == s512.S512_ERR_TIMEOUT
+        assert np.array_equal(hk, k0.cpu().numpy())
+        k, v = k0.clone(), v0.clone()
+        with pytest.raises(s512.Sort512Error) as e:
+            s512.partition_kv(k, v, 0, n - 1, 0)
+        assert e.value.code == s512.S512_ERR_TIMEOUT
+        assert torch.equal(k, k0) and torch.equal(v, v0)
+        d = workloads.uniform01_torch(n, 7)
+        d0 = d.clone()
+        with pytest.raises(s512.Sort512Error) as e:
+            s512.partition(d, 0, n - 1, 0.5)
+        assert e.value.code == s512.S512_ERR_TIMEOUT
+        assert torch.equal(d, d0)
+    finally:
+        s512.set_config(fault_inject=0)
+    torch.cuda.synchronize()  # the context is intact
+    k = k0.clone()
+    lim = s512.partition(k, 0, n - 1, 0)
+    assert lim == int((k0 <= 0).sum())

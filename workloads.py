@@ -208,3 +208,47 @@ def gauss_mix_i32_torch(n: int, seed: int = 0, device="cuda"):
     """Mixture of 8 Gaussians rounded to int32 (means U[-1e6,1e6], sigmas U[1,1e3])."""
     torch = _torch()
     return torch.round(double_dist_torch("gauss_mix", n, seed, device)).to(torch.int32)
+
+
+# ---------------------------------------------------------------------------
+# checks used by the benchmark at full size
+
+def order_keys_torch(t):
+    """int64 keys whose signed order is the sort order of t (IEEE total order
+    for float64: -0.0 before +0.0, NaNs at the ends by sign)."""
+    torch = _torch()
+    if t.dtype == torch.float64:
+        b = t.view(torch.int64)
+        return b ^ ((b >> 63) & 0x7FFFFFFFFFFFFFFF)
+    return t.to(torch.int64)
+
+
+def multiset_fingerprint_torch(*arrays):
+    """An order-independent fingerprint of the multiset of rows (one element
+    of each array per row): two wrapping 64-bit sums of differently mixed
+    splitmix64 finalisers of the row's bits.  Equal multisets give equal
+    fingerprints; a dropped, duplicated or altered element changes them with
+    overwhelming probability."""
+    torch = _torch()
+
+    def lsr(x, s):
+        return (x >> s) & ((1 << (64 - s)) - 1)
+
+    def mix(z):
+        z = z + _u64(_G)
+        z = (z ^ lsr(z, 30)) * _u64(_C1)
+        z = (z ^ lsr(z, 27)) * _u64(_C2)
+        return z ^ lsr(z, 31)
+
+    row = None
+    for a in arrays:
+        b = a.view(torch.int64) if a.element_size() == 8 else a.view(torch.int32).to(torch.int64)
+        row = b if row is None else mix(row) ^ b
+    h1 = mix(row)
+    h2 = mix(h1 ^ 0x5851F42D4C957F2D)
+    return int(h1.sum().item()), int(h2.sum().item())
+
+
+def is_sorted_torch(t) -> bool:
+    k = order_keys_torch(t)
+    return bool((k[1:] >= k[:-1]).all().item()) if k.numel() > 1 else True
