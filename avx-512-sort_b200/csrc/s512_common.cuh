@@ -79,6 +79,8 @@ struct Raw {
     __device__ __forceinline__ K load(size_t i) const { return __ldg(in + i); }
     __device__ __forceinline__ void store(size_t i, K k) const { out[i] = k; }
     __host__ __device__ const void* arr(int) const { return in; }
+    // the same codec reading other arrays (e.g. the caller's page-locked host memory)
+    Raw rebased(const void* const* a) const { return Raw{static_cast<const K*>(a[0]), out}; }
     __device__ __forceinline__ K decode(const unsigned char* buf, uint32_t i, uint32_t) const {
         return reinterpret_cast<const K*>(buf)[i];
     }
@@ -93,6 +95,7 @@ struct CodecI32 {
     __device__ __forceinline__ uint32_t load(size_t i) const { return enc_i32(__ldg(in + i)); }
     __device__ __forceinline__ void store(size_t i, uint32_t k) const { out[i] = dec_i32(k); }
     __host__ __device__ const void* arr(int) const { return in; }
+    CodecI32 rebased(const void* const* a) const { return CodecI32{static_cast<const int*>(a[0]), out}; }
     __device__ __forceinline__ uint32_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
         return enc_i32(reinterpret_cast<const int*>(buf)[i]);
     }
@@ -107,6 +110,9 @@ struct CodecF64 {
     __device__ __forceinline__ uint64_t load(size_t i) const { return enc_f64_bits(__ldg(in + i)); }
     __device__ __forceinline__ void store(size_t i, uint64_t k) const { out[i] = dec_f64_bits(k); }
     __host__ __device__ const void* arr(int) const { return in; }
+    CodecF64 rebased(const void* const* a) const {
+        return CodecF64{static_cast<const unsigned long long*>(a[0]), out};
+    }
     __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
         return enc_f64_bits(reinterpret_cast<const unsigned long long*>(buf)[i]);
     }
@@ -121,6 +127,9 @@ struct CodecKV {
     int* __restrict__ kout;
     int* __restrict__ vout;
     __host__ __device__ const void* arr(int k) const { return k ? (const void*)vin : (const void*)kin; }
+    CodecKV rebased(const void* const* a) const {
+        return CodecKV{static_cast<const int*>(a[0]), static_cast<const int*>(a[1]), kout, vout};
+    }
     __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t tile) const {
         return enc_kv(reinterpret_cast<const int*>(buf)[i], reinterpret_cast<const int*>(buf + (size_t)tile * 4)[i]);
     }
@@ -141,6 +150,9 @@ struct CodecI64 {
     __device__ __forceinline__ uint64_t load(size_t i) const { return __ldg(in + i) ^ 0x8000000000000000ull; }
     __device__ __forceinline__ void store(size_t i, uint64_t k) const { out[i] = k ^ 0x8000000000000000ull; }
     __host__ __device__ const void* arr(int) const { return in; }
+    CodecI64 rebased(const void* const* a) const {
+        return CodecI64{static_cast<const unsigned long long*>(a[0]), out};
+    }
     __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
         return reinterpret_cast<const unsigned long long*>(buf)[i] ^ 0x8000000000000000ull;
     }
@@ -164,6 +176,9 @@ struct CodecKVPairs {
         out[i] = ((unsigned long long)val << 32) | key;
     }
     __host__ __device__ const void* arr(int) const { return in; }
+    CodecKVPairs rebased(const void* const* a) const {
+        return CodecKVPairs{static_cast<const unsigned long long*>(a[0]), out};
+    }
     __device__ __forceinline__ uint64_t decode(const unsigned char* buf, uint32_t i, uint32_t) const {
         return enc(reinterpret_cast<const unsigned long long*>(buf)[i]);
     }

@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(LR_THREADS) root_grad_kernel(const K* __restri
 template <typename K>
 static int root_grad(const void* d_keys, uint32_t m, const float* theta, float* loss, float* grad, cudaStream_t st) {
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     float* buf = (float*)C->get("lr_diag", (2 * LR_ROOT + 1) * sizeof(float));
@@ -65,7 +65,7 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
         return S512_ERR_ARG;
     }
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     K* samples = (K*)C->get("lr_fit_samples", (size_t)SAMPLE_N * KB);

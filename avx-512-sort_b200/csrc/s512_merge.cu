@@ -68,7 +68,7 @@ static int merge_entry(T* data, size_t n, size_t middle, int flags, void* stream
     if (!data) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     S512_HOST_PTR(host, data, flags);
@@ -99,7 +99,7 @@ static int sort_by_chunks(T* data, size_t n, int nparts, int flags, void* stream
     if (!data || nparts < 1) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     S512_HOST_PTR(host, data, flags);
     T* d = data;

@@ -8,14 +8,15 @@
 namespace s512 {
 
 // Tile shapes of the partition kernel per key size: levels with many segments
-// (PartShape), and a level that is one whole array (PartShapeOne), where a
-// bigger tile halves the look-back walks of the single chain.
+// (PartShape), and a level that is one whole array (PartShapeOne).  512
+// threads and 24-32 KB of keys per tile: two blocks (2 x ~90 KB of shared
+// memory) share an SM.
 template <typename K> struct PartShape;
-template <> struct PartShape<uint32_t> { static constexpr int THREADS = 512, IPT = 16; };
+template <> struct PartShape<uint32_t> { static constexpr int THREADS = 512, IPT = 12; };
 template <> struct PartShape<uint64_t> { static constexpr int THREADS = 512, IPT = 8; };
 template <typename K> struct PartShapeOne;
-template <> struct PartShapeOne<uint32_t> { static constexpr int THREADS = 1024, IPT = 16; };
-template <> struct PartShapeOne<uint64_t> { static constexpr int THREADS = 1024, IPT = 12; };
+template <> struct PartShapeOne<uint32_t> { static constexpr int THREADS = 512, IPT = 12; };
+template <> struct PartShapeOne<uint64_t> { static constexpr int THREADS = 512, IPT = 8; };
 
 // ---------------------------------------------------------------------------
 // leaf launches per class
@@ -122,6 +123,26 @@ static bool codec_aligned(const C& c) {
 }
 
 // ---------------------------------------------------------------------------
+// The first partition level of a host-pointer sort, fed while the caller's
+// page-locked arrays are still being copied in: the sample is read from the
+// host arrays themselves (through their device addresses), and the
+// partition kernel runs once per chunk, each launch waiting for its chunk's
+// copy.  Chunks are whole tiles of that level.
+struct HostFeed {
+    const void* mapped[2];      // device addresses of the caller's host arrays
+    uint32_t nchunks;
+    uint64_t chunk_keys;        // keys per chunk (a multiple of the level's tile)
+    const cudaEvent_t* ready;   // ready[c]: chunk c is on the device
+};
+
+// The stream waits for every chunk (a sort that does not consume the feed).
+static inline int wait_feed(const HostFeed* feed, cudaStream_t st) {
+    if (!feed) return S512_OK;
+    for (uint32_t c = 0; c < feed->nchunks; ++c) S512_CUDA_TRY(cudaStreamWaitEvent(st, feed->ready[c], 0));
+    return S512_OK;
+}
+
+// ---------------------------------------------------------------------------
 // One partition level: sample -> sort sample -> splitters -> partition -> plan.
 template <typename K, typename InCodec>
 struct Level {
@@ -139,7 +160,8 @@ struct Level {
 template <typename K, typename InCodec, typename UserOut, typename Shape = PartShape<K>>
 static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, size_t n, cudaStream_t st,
                      LevelCtl* ctl, LevelCtl* next_ctl_dev, SegDesc* next_segs, uint32_t next_cap,
-                     PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl, bool learned) {
+                     PhaseTimer& tm, s512_stats& S, LevelCtl* host_ctl, bool learned,
+                     const HostFeed* feed = nullptr) {
     constexpr int KB = sizeof(K);
     const uint32_t nsegs = L.nsegs;
     int rc;
@@ -148,8 +170,6 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     K* samples = (K*)C.get("samples", (size_t)nsegs * SAMPLE_N * KB);
     SplitSet<K>* splits = (SplitSet<K>*)C.get("splits", (size_t)nsegs * sizeof(SplitSet<K>));
     uint64_t* counts = (uint64_t*)C.get("counts", (size_t)nsegs * NB * sizeof(uint64_t));
-    unsigned long long* status =
-        (unsigned long long*)C.get("status", (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long));
     const uint32_t item_cap = nsegs * NB + (uint32_t)(n / COPY_CHUNK) + 16;
     LeafItem<K>* items[NCLASS + 1];
     {
@@ -157,17 +177,17 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         if (!base) return S512_ERR_ALLOC;
         for (int c = 0; c <= NCLASS; ++c) items[c] = (LeafItem<K>*)(base + (size_t)c * item_cap * sizeof(LeafItem<K>));
     }
-    uint32_t* chain = (uint32_t*)C.get("chain", (size_t)nsegs * sizeof(uint32_t));
     LearnedSet<K>* lsets = learned ? (LearnedSet<K>*)C.get("lsets", (size_t)nsegs * sizeof(LearnedSet<K>)) : nullptr;
-    if (!samples || !splits || !counts || !status || !chain || (learned && !lsets)) return S512_ERR_ALLOC;
+    if (!samples || !splits || !counts || (learned && !lsets)) return S512_ERR_ALLOC;
 
     const int t0 = tm.mark();
     S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
-    S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
     S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
-    S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
     const uint64_t seed = config().seed + 0x9E3779B97F4A7C15ull * (uint64_t)(level + 1);
-    sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed, KB);
+    if (feed)  // the caller's host arrays, read where they are
+        sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in.rebased(feed->mapped), L.segs, nsegs, samples, seed, KB);
+    else
+        sample_kernel<InCodec><<<nsegs, 256, 0, st>>>(L.in, L.segs, nsegs, samples, seed, KB);
     S512_LAUNCH_CHECK();
     {
         auto fn = sample_sort_kernel<K>;
@@ -203,24 +223,44 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     pa.tile_seg = L.tile_seg;
     pa.splits = splits;
     pa.out = L.out;
-    pa.status = status;
-    pa.bucket_counts = counts;
+    pa.fill = (unsigned long long*)counts;
     pa.ctl = ctl;
     pa.ntiles = L.ntiles_host;
     pa.ntiles_dev = L.ntiles_dev;
+    pa.tile_first = 0;
+    pa.tile_counter = &ctl->tile_counter;
     pa.nsegs = nsegs;
     pa.tma = (L.aligned && codec_aligned(L.in)) ? 1 : 0;
-    pa.chain = chain;
     pa.learned = lsets;
-    // the status array has one spare slot past the level's tiles, never written
-    pa.inject_slot = (fault & S512_FAULT_TIMEOUT) ? L.ntiles_bound : 0xFFFFFFFFu;
+    pa.inject_timeout = (fault & S512_FAULT_TIMEOUT) ? 1 : 0;
     auto pfn = partition_kernel<K, InCodec, Shape::THREADS, Shape::IPT>;
     const size_t psmem = sizeof(PartSmem<K, Shape::THREADS, Shape::IPT>);
     int pgrid = 0;
     S512_CUDA_TRY(launch_persistent(C, pfn, Shape::THREADS, psmem, st, 0, &pgrid));
-    pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
-    S512_LAUNCH_CHECK();
-    S.kernel_launches += 1;
+    if (feed) {
+        // one launch per chunk of the input, each after its chunk's copy
+        constexpr uint32_t TILE = Shape::THREADS * Shape::IPT;
+        uint32_t* cctr = (uint32_t*)C.get("chunk_ctr", (size_t)feed->nchunks * sizeof(uint32_t));
+        if (!cctr) return S512_ERR_ALLOC;
+        S512_CUDA_TRY(cudaMemsetAsync(cctr, 0, (size_t)feed->nchunks * sizeof(uint32_t), st));
+        const uint32_t tpc = (uint32_t)(feed->chunk_keys / TILE);
+        for (uint32_t c = 0; c < feed->nchunks; ++c) {
+            PartArgs<K> pc = pa;
+            pc.tile_first = c * tpc;
+            pc.ntiles = (c + 1) * tpc < L.ntiles_host ? (c + 1) * tpc : L.ntiles_host;
+            pc.tile_counter = cctr + c;
+            const uint32_t claims = (pc.ntiles - pc.tile_first + CLAIM_GROUP_ONE_SEG - 1) / CLAIM_GROUP_ONE_SEG;
+            const int g = pgrid < (int)claims ? pgrid : (int)claims;
+            S512_CUDA_TRY(cudaStreamWaitEvent(st, feed->ready[c], 0));
+            pfn<<<g, Shape::THREADS, psmem, st>>>(pc, L.in);
+            S512_LAUNCH_CHECK();
+        }
+        S.kernel_launches += feed->nchunks;
+    } else {
+        pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
+        S512_LAUNCH_CHECK();
+        S.kernel_launches += 1;
+    }
     const int t2 = tm.mark();
 
     PlanArgs<K> pl;
@@ -242,7 +282,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     S.kernel_launches += 1;
 
     if (host_ctl->err & DEV_ERR_TIMEOUT) {
-        set_error("partition look-back wait timed out at level %d", level);
+        set_error("partition wait timed out at level %d", level);
         return S512_ERR_TIMEOUT;
     }
     if (host_ctl->err & DEV_ERR_OVERFLOW) {
@@ -264,9 +304,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
         exact_regions_kernel<K><<<nsegs, NB, 0, st>>>(splits, counts, nsegs);
         S512_LAUNCH_CHECK();
         S512_CUDA_TRY(cudaMemsetAsync(ctl, 0, sizeof(LevelCtl), st));
-        S512_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(L.ntiles_bound + 1) * NB * sizeof(unsigned long long), st));
         S512_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)nsegs * NB * sizeof(uint64_t), st));
-        S512_CUDA_TRY(cudaMemsetAsync(chain, 0, (size_t)nsegs * sizeof(uint32_t), st));
         pfn<<<pgrid, Shape::THREADS, psmem, st>>>(pa, L.in);
         S512_LAUNCH_CHECK();
         plan_kernel<K><<<nsegs, NB, 0, st>>>(pl, nsegs);
@@ -277,7 +315,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     }
     if (host_ctl->err) {
         if (host_ctl->err & DEV_ERR_TIMEOUT) {
-            set_error("partition look-back wait timed out at level %d", level);
+            set_error("partition wait timed out at level %d", level);
             return S512_ERR_TIMEOUT;
         }
         set_error("partition level %d reported device error 0x%x", level, host_ctl->err);
@@ -337,7 +375,8 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
 // aligned for the bulk copy).
 template <typename K, typename UserIn, typename UserOut>
 static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint32_t nsegs0, uint64_t keys0,
-                      cudaStream_t st, PhaseTimer& tm, s512_stats& S, bool whole, bool learned = false) {
+                      cudaStream_t st, PhaseTimer& tm, s512_stats& S, bool whole, bool learned = false,
+                      const HostFeed* feed = nullptr) {
     constexpr int KB = sizeof(K);
     using Shape = PartShape<K>;
     constexpr int TILE = Shape::THREADS * Shape::IPT;
@@ -388,8 +427,10 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         L0.ntiles_bound = bound;
         L0.aligned = false;  // segment starts are wherever the caller's segments start
     }
+    if (!single) S512_TRY_RC(wait_feed(feed, st));  // (only a whole array is fed chunk by chunk)
     int rc = single ? run_level<K, UserIn, UserOut, PartShapeOne<K>>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1],
-                                                                      segbuf[1], next_cap, tm, S, host_ctl, learned)
+                                                                      segbuf[1], next_cap, tm, S, host_ctl, learned,
+                                                                      feed)
                     : run_level<K, UserIn, UserOut>(C, L0, 0, uout, keys0, st, &ctls[0], &ctls[1], segbuf[1],
                                                     next_cap, tm, S, host_ctl, learned);
     if (rc) return rc;
@@ -448,7 +489,8 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
 
 // The whole pipeline for one array of n > leaf_max keys.
 template <typename K, typename UserIn, typename UserOut>
-static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned) {
+static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned,
+                         const HostFeed* feed = nullptr) {
     constexpr int TILE = PartShapeOne<K>::THREADS * PartShapeOne<K>::IPT;  // a single segment
     s512_stats& S = thread_stats();
     PhaseTimer tm(st, config().collect_stats != 0);
@@ -463,7 +505,7 @@ static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStre
     s0.tile_start = 0;
     s0.ntiles = (uint32_t)((n + TILE - 1) / TILE);
     S512_CUDA_TRY(cudaMemcpyAsync(seg0, &s0, sizeof(SegDesc), cudaMemcpyHostToDevice, st));
-    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S, true, learned);
+    int rc = run_levels<K, UserIn, UserOut>(C, uin, uout, seg0, 1, n, st, tm, S, true, learned, feed);
     if (rc) return rc;
     const int tend = tm.mark();
     if (tm.on()) S.total_ms = tm.ms(tstart, tend);
@@ -474,10 +516,12 @@ static int sort_pipeline(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStre
 // Entry: sort `n` keys read through uin and written through uout (same
 // positions; device memory).
 template <typename K, typename UserIn, typename UserOut>
-static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned = false) {
+static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream_t st, bool learned = false,
+                       const HostFeed* feed = nullptr) {
     s512_stats& S = thread_stats();
     memset(&S, 0, sizeof(S));
     S.key_bytes = sizeof(K);
+    if (n <= leaf_max(sizeof(K))) S512_TRY_RC(wait_feed(feed, st));  // no partition level to feed
     if (n <= 1) {
         if (n == 1) {
             // still route through the codec so in != out works
@@ -496,14 +540,64 @@ static int sort_device(DevCtx& C, UserIn uin, UserOut uout, size_t n, cudaStream
         if (tm.on()) S.total_ms = tm.ms(a, b);
         return rc;
     }
-    return sort_pipeline<K, UserIn, UserOut>(C, uin, uout, n, st, learned);
+    return sort_pipeline<K, UserIn, UserOut>(C, uin, uout, n, st, learned, feed);
 }
 
 // ---------------------------------------------------------------------------
-// Host-pointer staging: copy to a device buffer, run `fn`, copy back.
-struct HostStage {
-    void* dev[2] = {nullptr, nullptr};
-};
+// Host-pointer calls: the caller's arrays are copied to device buffers of the
+// stream's pool, sorted there and copied back.
+
+// Page-locked host arrays at least this large are copied in chunks that the
+// first partition level consumes as they land.
+constexpr size_t HOST_CHUNKED_MIN_BYTES = 16u << 20;
+constexpr uint32_t HOST_CHUNKS = 32;
+
+// Copy n elements of narr host arrays (esz bytes each) into the device
+// buffers dev[].  Page-locked arrays that a sort of K keys would partition
+// go in chunks on the pool's copy stream, with *feed describing them for the
+// first level (*chunked set); anything else is one copy per array on st.
+template <typename K>
+static int copy_in(DevCtx& C, int narr, void* const* host, void* const* dev, size_t esz, size_t n, bool pinned,
+                   cudaStream_t st, HostFeed* feed, bool* chunked) {
+    *chunked = false;
+    const void* mapped[2] = {nullptr, nullptr};
+    bool can = pinned && n > leaf_max(sizeof(K)) && n * esz * narr >= HOST_CHUNKED_MIN_BYTES;
+    for (int k = 0; can && k < narr; ++k) {
+        mapped[k] = mapped_host_address(host[k]);
+        can = mapped[k] != nullptr;
+    }
+    if (!can) {
+        for (int k = 0; k < narr; ++k)
+            S512_CUDA_TRY(cudaMemcpyAsync(dev[k], host[k], n * esz, cudaMemcpyHostToDevice, st));
+        return S512_OK;
+    }
+    constexpr uint64_t TILE = (uint64_t)PartShapeOne<K>::THREADS * PartShapeOne<K>::IPT;
+    const uint64_t per = (n + HOST_CHUNKS - 1) / HOST_CHUNKS;
+    const uint64_t chunk = (per + TILE - 1) / TILE * TILE;
+    const uint32_t nchunks = (uint32_t)((n + chunk - 1) / chunk);
+    S512_CUDA_TRY(C.copy_resources(nchunks + 1));
+    // the copies start after the work already queued on st (which may still
+    // read the same device buffers)
+    cudaEvent_t start = C.events[nchunks];
+    S512_CUDA_TRY(cudaEventRecord(start, st));
+    S512_CUDA_TRY(cudaStreamWaitEvent(C.copy_stream, start, 0));
+    for (uint32_t c = 0; c < nchunks; ++c) {
+        const uint64_t off = (uint64_t)c * chunk;
+        const uint64_t len = n - off < chunk ? n - off : chunk;
+        for (int k = 0; k < narr; ++k)
+            S512_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(dev[k]) + off * esz,
+                                          static_cast<const char*>(host[k]) + off * esz, len * esz,
+                                          cudaMemcpyHostToDevice, C.copy_stream));
+        S512_CUDA_TRY(cudaEventRecord(C.events[c], C.copy_stream));
+    }
+    feed->mapped[0] = mapped[0];
+    feed->mapped[1] = mapped[1];
+    feed->nchunks = nchunks;
+    feed->chunk_keys = chunk;
+    feed->ready = C.events.data();
+    *chunked = true;
+    return S512_OK;
+}
 
 // learned splitters for this call: the flag wins over the configuration
 static inline bool use_learned(int flags) {
@@ -512,9 +606,12 @@ static inline bool use_learned(int flags) {
     return config().splitter_mode == S512_SPLIT_LEARNED;
 }
 
-static int finish_call(CallGuard& g, cudaStream_t st, int flags, bool host) {
+// A call returns at once with S512_ASYNC when its data is device memory or
+// page-locked host memory (the caller synchronises the stream before reading
+// the result); pageable host memory is always waited for.
+static int finish_call(CallGuard& g, cudaStream_t st, int flags, bool host, bool host_pinned = false) {
     g.finish();
-    if (host || !(flags & S512_ASYNC)) S512_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!(flags & S512_ASYNC) || (host && !host_pinned)) S512_CUDA_TRY(cudaStreamSynchronize(st));
     return S512_OK;
 }
 

@@ -52,6 +52,8 @@ void* DevCtx::get(const char* name, size_t bytes) {
     auto it = bufs.find(name);
     if (it != bufs.end()) {
         if (it->second.second >= bytes) return it->second.first;
+        // the old buffer may still be read by this stream's queued work
+        cudaStreamSynchronize(stream);
         cudaFree(it->second.first);
         bufs.erase(it);
     }
@@ -67,7 +69,10 @@ void* DevCtx::get(const char* name, size_t bytes) {
 
 void* DevCtx::host_pinned(size_t bytes) {
     if (pinned_bytes >= bytes) return pinned;
-    if (pinned) cudaFreeHost(pinned);
+    if (pinned) {
+        cudaStreamSynchronize(stream);
+        cudaFreeHost(pinned);
+    }
     pinned = nullptr;
     pinned_bytes = 0;
     if (cudaMallocHost(&pinned, bytes) != cudaSuccess) {
@@ -85,11 +90,33 @@ void DevCtx::release_all() {
     if (pinned) cudaFreeHost(pinned);
     pinned = nullptr;
     pinned_bytes = 0;
+    for (auto e : events) cudaEventDestroy(e);
+    events.clear();
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    copy_stream = nullptr;
+}
+
+cudaError_t DevCtx::copy_resources(size_t n) {
+    if (!copy_stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            copy_stream = nullptr;
+            return e;
+        }
+    }
+    while (events.size() < n) {
+        cudaEvent_t ev;
+        cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+        events.push_back(ev);
+    }
+    return cudaSuccess;
 }
 
 cudaError_t DevCtx::prepare(const void* fn, size_t smem) {
-    auto it = smem_set.find(fn);
-    if (it != smem_set.end() && it->second >= smem) return cudaSuccess;
+    std::lock_guard<std::mutex> lk(sh->mu);
+    auto it = sh->smem_set.find(fn);
+    if (it != sh->smem_set.end() && it->second >= smem) return cudaSuccess;
     // the 48 KB default covers static + dynamic shared memory together
     cudaFuncAttributes fa;
     cudaError_t ea = cudaFuncGetAttributes(&fa, fn);
@@ -102,15 +129,16 @@ cudaError_t DevCtx::prepare(const void* fn, size_t smem) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess) return e;
     }
-    smem_set[fn] = smem;
-    occ.erase(fn);
+    sh->smem_set[fn] = smem;
+    sh->occ.erase(fn);
     return cudaSuccess;
 }
 
 int DevCtx::persistent_grid(const void* fn, int threads, size_t smem) {
-    auto it = occ.find(fn);
+    std::lock_guard<std::mutex> lk(sh->mu);
+    auto it = sh->occ.find(fn);
     int per_sm;
-    if (it != occ.end()) {
+    if (it != sh->occ.end()) {
         per_sm = it->second;
     } else {
         per_sm = 0;
@@ -119,15 +147,16 @@ int DevCtx::persistent_grid(const void* fn, int threads, size_t smem) {
             per_sm = 1;
         }
         if (per_sm < 1) per_sm = 1;
-        occ[fn] = per_sm;
+        sh->occ[fn] = per_sm;
     }
     return per_sm * sms;
 }
 
 static std::mutex g_ctx_mu;
-static std::map<int, DevCtx*> g_ctx;
+static std::map<int, DevShared*> g_dev;
+static std::map<std::pair<int, cudaStream_t>, DevCtx*> g_ctx;
 
-DevCtx* current_ctx(int* status) {
+DevCtx* current_ctx(int* status, cudaStream_t st) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
@@ -136,64 +165,100 @@ DevCtx* current_ctx(int* status) {
         return nullptr;
     }
     std::lock_guard<std::mutex> lk(g_ctx_mu);
-    auto it = g_ctx.find(dev);
+    auto it = g_ctx.find({dev, st});
     if (it != g_ctx.end()) {
         *status = S512_OK;
         return it->second;
     }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
-        cudaGetLastError();
-        set_error("cudaGetDeviceProperties failed");
-        *status = S512_ERR_CUDA;
-        return nullptr;
-    }
-    if (prop.major < 10) {
-        set_error("device %d (%s, sm_%d%d) is not an sm_100 part; this library is built for sm_100a only", dev,
-                  prop.name, prop.major, prop.minor);
-        *status = S512_ERR_UNSUPPORTED;
-        return nullptr;
+    DevShared* sh;
+    auto dit = g_dev.find(dev);
+    if (dit != g_dev.end()) {
+        sh = dit->second;
+    } else {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaGetDeviceProperties failed");
+            *status = S512_ERR_CUDA;
+            return nullptr;
+        }
+        if (prop.major < 10) {
+            set_error("device %d (%s, sm_%d%d) is not an sm_100 part; this library is built for sm_100a only", dev,
+                      prop.name, prop.major, prop.minor);
+            *status = S512_ERR_UNSUPPORTED;
+            return nullptr;
+        }
+        sh = new DevShared();
+        sh->dev = dev;
+        sh->sms = prop.multiProcessorCount;
+        sh->smem_optin = prop.sharedMemPerBlockOptin;
+        g_dev[dev] = sh;
     }
     DevCtx* c = new DevCtx();
+    c->sh = sh;
     c->dev = dev;
-    c->sms = prop.multiProcessorCount;
-    c->smem_optin = prop.sharedMemPerBlockOptin;
-    g_ctx[dev] = c;
+    c->sms = sh->sms;
+    c->smem_optin = sh->smem_optin;
+    c->stream = st;
+    g_ctx[{dev, st}] = c;
     *status = S512_OK;
     return c;
 }
 
-CallGuard::CallGuard(DevCtx* c, cudaStream_t st) : c_(c), st_(st), lk_(c->mu) {
-    if (c_->last_done) cudaStreamWaitEvent(st_, c_->last_done, 0);
+// every pool of the current device
+static void release_device_pools() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    std::vector<DevCtx*> mine;
+    {
+        std::lock_guard<std::mutex> lk(g_ctx_mu);
+        for (auto& kv : g_ctx)
+            if (kv.first.first == dev) mine.push_back(kv.second);
+    }
+    cudaDeviceSynchronize();
+    for (DevCtx* c : mine) {
+        std::lock_guard<std::mutex> lk(c->mu);
+        c->release_all();
+    }
 }
 
-void CallGuard::finish() {
-    if (!c_->last_done) cudaEventCreateWithFlags(&c_->last_done, cudaEventDisableTiming);
-    cudaEventRecord(c_->last_done, st_);
-}
+CallGuard::CallGuard(DevCtx* c, cudaStream_t) : lk_(c->mu) {}
 
 CallGuard::~CallGuard() {}
 
 int pointer_kind(const void* p, int flags) {
-    if (flags & S512_PTR_HOST) return 1;
-    if (flags & S512_PTR_DEVICE) return 2;
+    if (flags & S512_PTR_DEVICE) return PTR_DEVICE_MEM;
     cudaPointerAttributes at;
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
         cudaGetLastError();
-        return 1;
+        return PTR_PAGEABLE;
     }
-    if (at.type == cudaMemoryTypeManaged) return 2;
-    if (at.type != cudaMemoryTypeDevice) return 1;
+    if (at.type == cudaMemoryTypeHost) return at.devicePointer ? PTR_PINNED : PTR_PAGEABLE;
+    if (flags & S512_PTR_HOST) return PTR_PAGEABLE;
+    if (at.type == cudaMemoryTypeManaged) return PTR_DEVICE_MEM;
+    if (at.type != cudaMemoryTypeDevice) return PTR_PAGEABLE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
-        return 0;
+        return PTR_OTHER_DEVICE;
     }
     if (at.device != dev) {
         set_error("pointer %p is memory of device %d, the current device is %d", p, at.device, dev);
-        return 0;
+        return PTR_OTHER_DEVICE;
     }
-    return 2;
+    return PTR_DEVICE_MEM;
+}
+
+const void* mapped_host_address(const void* p) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
 }
 
 }  // namespace s512
@@ -225,11 +290,9 @@ const char* s512_last_error_string(void) { return s512::g_err; }
 
 int s512_release_scratch(void) {
     int st = 0;
-    s512::DevCtx* c = s512::current_ctx(&st);
+    s512::DevCtx* c = s512::current_ctx(&st, nullptr);
     if (!c) return st;
-    std::lock_guard<std::mutex> lk(c->mu);
-    cudaDeviceSynchronize();
-    c->release_all();
+    s512::release_device_pools();
     return S512_OK;
 }
 

@@ -189,7 +189,7 @@ static int segsort_entry(int dt, void* keys, void* values, size_t elem_bytes, co
     if (!keys || !offsets || (dt == DT_KV && !values)) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     S512_HOST_PTR(host, keys, flags);
@@ -334,7 +334,7 @@ int s512_segsort_tune(int dtype, const size_t* d_offsets, size_t nseg, double* b
     if (dtype < 0 || dtype >= NUM_DT || !d_offsets || nseg == 0) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     if (pointer_kind(d_offsets, 0) != 2) {
         set_error("s512_segsort_tune: offsets must be device memory");
@@ -369,7 +369,7 @@ int s512_segsort_plan_create(s512_segsort_plan** out, int dtype, void* keys, voi
     }
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     Plan* p = new Plan();
     memset(p, 0, sizeof(Plan));
@@ -446,7 +446,7 @@ int s512_segsort_plan_launch(s512_segsort_plan* plan, void* stream) {
     if (!p || !p->exec) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     s512_stats& S = thread_stats();

@@ -65,13 +65,14 @@ struct SlotRed {
 };
 
 // Shared memory of block_slot_sort for a block of THREADS x IPT keys: the
-// key buffer (padded for the block sort when that runs inline, INLINE) and
-// the counters.
+// key buffer (padded for the block sort when that runs inline, INLINE), the
+// counters, and one bit per slot that marks slots of more than one key.
 template <typename K, int THREADS, int IPT, bool INLINE = true>
 struct SlotSmem {
     static constexpr uint32_t S = (uint32_t)THREADS * IPT;
     static constexpr size_t keys_bytes = ((size_t)(INLINE ? padded_len(S) : S) * sizeof(K) + 15) & ~(size_t)15;
-    static constexpr size_t bytes = keys_bytes + (size_t)S * sizeof(uint32_t);
+    static constexpr size_t ctr_bytes = (size_t)S * sizeof(uint32_t);
+    static constexpr size_t bytes = keys_bytes + ctr_bytes + (size_t)S / 8;
 };
 
 // Sort the c <= THREADS*IPT keys held striped in key[] (element
@@ -92,9 +93,11 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
                                 unsigned char* smem, SlotRed<K>& red) {
     constexpr uint32_t S = (uint32_t)THREADS * IPT;
     constexpr int NW = THREADS / 32;
-    static_assert(IPT % 4 == 0, "counters are read four at a time");
+    static_assert(IPT % 4 == 0 && 32 % IPT == 0, "counters are read four at a time, slot bits in whole words");
+    using SM = SlotSmem<K, THREADS, IPT, INLINE_FALLBACK>;
     K* s = reinterpret_cast<K*>(smem);
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SlotSmem<K, THREADS, IPT, INLINE_FALLBACK>::keys_bytes);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes);
+    uint32_t* multi = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes + SM::ctr_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
     // 1. bounds of the bucket; counters zeroed
@@ -189,13 +192,24 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
         // counts -> slot starts (the counters are read again rather than kept
         // in registers across the barrier)
         uint32_t run = before + inc - sum;
+        uint32_t mbits = 0;  // bit r: slot tid*IPT + r holds more than one key
 #pragma unroll
         for (int r = 0; r < IPT; r += 4) {
             uint4 q = *reinterpret_cast<const uint4*>(&ctr[tid * IPT + r]);
+            mbits |= ((q.x > 1u) ? 1u : 0u) << r | ((q.y > 1u) ? 1u : 0u) << (r + 1) |
+                     ((q.z > 1u) ? 1u : 0u) << (r + 2) | ((q.w > 1u) ? 1u : 0u) << (r + 3);
             const uint32_t s0 = run, s1 = s0 + q.x, s2 = s1 + q.y, s3 = s2 + q.z;
             run = s3 + q.w;
             q = make_uint4(s0, s1, s2, s3);
             *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = q;
+        }
+        {
+            // the bits of the 32/IPT threads that share a word of `multi`
+            constexpr int G = 32 / IPT;
+            uint32_t w = G > 1 ? mbits << ((lane % G) * IPT) : mbits;
+#pragma unroll
+            for (int d = 1; d < G; d <<= 1) w |= __shfl_xor_sync(0xFFFFFFFFu, w, d);
+            if (lane % G == 0) multi[(tid * IPT) >> 5] = w;
         }
         __syncthreads();
         // 4. deal the keys into their slots; afterwards ctr[j] is the end of slot j
@@ -205,10 +219,15 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
         }
         refill();
         __syncthreads();
-        // 5. rank each key inside its slot and write it to its final place
+        // 5. rank each key inside its slot and write it to its final place;
+        //    the key of a one-key slot is already there (rank p)
         for (uint32_t p = tid; p < c; p += THREADS) {
             const K x = s[p];
             const uint32_t j = f(x);
+            if (!((multi[j >> 5] >> (j & 31)) & 1u)) {
+                store(p, x);
+                continue;
+            }
             const uint32_t a = j ? ctr[j - 1] : 0u;
             const uint32_t e = ctr[j];
             uint32_t rank = a;

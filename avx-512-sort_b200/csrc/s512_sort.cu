@@ -18,7 +18,7 @@ using namespace s512;
 
 #define S512_ENTER(ctxvar, st)              \
     int status_ = S512_OK;                  \
-    DevCtx* ctxvar = current_ctx(&status_); \
+    DevCtx* ctxvar = current_ctx(&status_, st); \
     if (!ctxvar) return status_;            \
     CallGuard guard_(ctxvar, st)
 
@@ -37,15 +37,20 @@ int s512_sort_i32(int* data, size_t n, int flags, void* stream) {
         return finish_call(guard_, st, flags, host);
     }
     int* d = data;
+    HostFeed feed;
+    bool chunked = false;
     if (host) {
         d = (int*)C->get("stage0", n * sizeof(int));
         if (!d) return S512_ERR_ALLOC;
-        S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * sizeof(int), cudaMemcpyHostToDevice, st));
+        void* hp[1] = {data};
+        void* dp[1] = {d};
+        S512_TRY_RC(copy_in<uint32_t>(*C, 1, hp, dp, sizeof(int), n, host_pinned, st, &feed, &chunked));
     }
-    int rc = sort_device<uint32_t>(*C, CodecI32{d, d}, CodecI32{d, d}, n, st, use_learned(flags));
+    int rc = sort_device<uint32_t>(*C, CodecI32{d, d}, CodecI32{d, d}, n, st, use_learned(flags),
+                                   chunked ? &feed : nullptr);
     if (rc) return rc;
     if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-    return finish_call(guard_, st, flags, host);
+    return finish_call(guard_, st, flags, host, host_pinned);
 }
 
 int s512_sort_f64(double* data, size_t n, int flags, void* stream) {
@@ -60,15 +65,20 @@ int s512_sort_f64(double* data, size_t n, int flags, void* stream) {
         return finish_call(guard_, st, flags, host);
     }
     unsigned long long* d = (unsigned long long*)data;
+    HostFeed feed;
+    bool chunked = false;
     if (host) {
         d = (unsigned long long*)C->get("stage0", n * sizeof(double));
         if (!d) return S512_ERR_ALLOC;
-        S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        void* hp[1] = {data};
+        void* dp[1] = {d};
+        S512_TRY_RC(copy_in<uint64_t>(*C, 1, hp, dp, sizeof(double), n, host_pinned, st, &feed, &chunked));
     }
-    int rc = sort_device<uint64_t>(*C, CodecF64{d, d}, CodecF64{d, d}, n, st, use_learned(flags));
+    int rc = sort_device<uint64_t>(*C, CodecF64{d, d}, CodecF64{d, d}, n, st, use_learned(flags),
+                                   chunked ? &feed : nullptr);
     if (rc) return rc;
     if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * sizeof(double), cudaMemcpyDeviceToHost, st));
-    return finish_call(guard_, st, flags, host);
+    return finish_call(guard_, st, flags, host, host_pinned);
 }
 
 int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream) {
@@ -79,20 +89,28 @@ int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream) 
     S512_HOST_PTR(host, keys, flags);
     int* dk = keys;
     int* dv = values;
+    HostFeed feed;
+    bool chunked = false;
+    bool pinned_both = false;
     if (host) {
+        // both arrays are host memory; both must be page-locked to be fed in chunks
+        S512_HOST_PTR(vhost, values, flags);
+        pinned_both = host_pinned && vhost && vhost_pinned;
         dk = (int*)C->get("stage0", n * sizeof(int));
         dv = (int*)C->get("stage1", n * sizeof(int));
         if (!dk || !dv) return S512_ERR_ALLOC;
-        S512_CUDA_TRY(cudaMemcpyAsync(dk, keys, n * sizeof(int), cudaMemcpyHostToDevice, st));
-        S512_CUDA_TRY(cudaMemcpyAsync(dv, values, n * sizeof(int), cudaMemcpyHostToDevice, st));
+        void* hp[2] = {keys, values};
+        void* dp[2] = {dk, dv};
+        S512_TRY_RC(copy_in<uint64_t>(*C, 2, hp, dp, sizeof(int), n, pinned_both, st, &feed, &chunked));
     }
-    int rc = sort_device<uint64_t>(*C, CodecKV{dk, dv, dk, dv}, CodecKV{dk, dv, dk, dv}, n, st, use_learned(flags));
+    int rc = sort_device<uint64_t>(*C, CodecKV{dk, dv, dk, dv}, CodecKV{dk, dv, dk, dv}, n, st, use_learned(flags),
+                                   chunked ? &feed : nullptr);
     if (rc) return rc;
     if (host) {
         S512_CUDA_TRY(cudaMemcpyAsync(keys, dk, n * sizeof(int), cudaMemcpyDeviceToHost, st));
         S512_CUDA_TRY(cudaMemcpyAsync(values, dv, n * sizeof(int), cudaMemcpyDeviceToHost, st));
     }
-    return finish_call(guard_, st, flags, host);
+    return finish_call(guard_, st, flags, host, pinned_both);
 }
 
 // ---- SmallSort16V / CoreSmallSortN ----------------------------------------

@@ -18,7 +18,7 @@ static int sort_words(T* data, size_t n, int flags, void* stream) {
     if (!data) return S512_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     int status = S512_OK;
-    DevCtx* C = current_ctx(&status);
+    DevCtx* C = current_ctx(&status, st);
     if (!C) return status;
     CallGuard guard(C, st);
     S512_HOST_PTR(host, data, flags);
@@ -30,15 +30,19 @@ static int sort_words(T* data, size_t n, int flags, void* stream) {
         }
     }
     unsigned long long* d = (unsigned long long*)data;
+    HostFeed feed;
+    bool chunked = false;
     if (host) {
         d = (unsigned long long*)C->get("stage0", n * 8);
         if (!d) return S512_ERR_ALLOC;
-        S512_CUDA_TRY(cudaMemcpyAsync(d, data, n * 8, cudaMemcpyHostToDevice, st));
+        void* hp[1] = {data};
+        void* dp[1] = {d};
+        S512_TRY_RC(copy_in<uint64_t>(*C, 1, hp, dp, 8, n, host_pinned, st, &feed, &chunked));
     }
-    int rc = sort_device<uint64_t>(*C, Codec{d, d}, Codec{d, d}, n, st, use_learned(flags));
+    int rc = sort_device<uint64_t>(*C, Codec{d, d}, Codec{d, d}, n, st, use_learned(flags), chunked ? &feed : nullptr);
     if (rc) return rc;
     if (host) S512_CUDA_TRY(cudaMemcpyAsync(data, d, n * 8, cudaMemcpyDeviceToHost, st));
-    return finish_call(guard, st, flags, host);
+    return finish_call(guard, st, flags, host, host_pinned);
 }
 
 }  // namespace s512

@@ -13,12 +13,12 @@
 //     equal to that value need no further sorting), which removes the
 //     reference's quadratic behaviour on few-distinct and sorted inputs;
 //   * the partition pass is out of place and "one sweep": every tile of keys
-//     computes its bucket histogram, publishes it, and learns the number of
-//     keys of each bucket in all earlier tiles from a decoupled look-back over
-//     per-tile status words, then scatters its keys through shared memory so
-//     global writes are coalesced.  Bucket b of a segment is written into a
-//     region whose capacity comes from the sample (a 6-sigma bound); a bucket
-//     that outgrows it is reported and the level is redone with exact counts;
+//     computes its bucket histogram, reserves its share of each bucket's
+//     output region with one atomic add per bucket, then scatters its keys
+//     through shared memory so global writes are coalesced.  Bucket b of a
+//     segment is written into a region whose capacity comes from the sample
+//     (a 6-sigma bound); a bucket that outgrows it is reported and the level
+//     is redone with exact counts;
 //   * buckets at most a leaf's capacity are sorted by the bitonic networks of
 //     s512_bitonic.cuh (one warp or one block per bucket, by size class) and
 //     written to their final place; larger buckets become the segments of the
@@ -35,9 +35,6 @@ constexpr int NB = 256;            // buckets per segment per pass (max)
 constexpr int SAMPLE_N = 16384;    // keys sampled per segment
 constexpr int COPY_CHUNK = 16384;  // equality buckets are copied in chunks of this size
 constexpr int SPLIT_SLOTS = 4096;  // value slots of the splitter lookup table
-constexpr unsigned long long ST_INC = 1ull << 63;  // status: inclusive prefix
-constexpr unsigned long long ST_AGG = 1ull << 62;  // status: tile aggregate only
-constexpr unsigned long long ST_VAL = (1ull << 62) - 1;
 
 // A segment to partition at some level.
 struct SegDesc {
@@ -66,13 +63,14 @@ struct SplitSet {
     uint32_t nuniq;
     uint32_t pad_;
     // Lookup table over the sample's value range: keys are clamped to
-    // [slot_map.lo, slot_hi] and mapped to SPLIT_SLOTS slots by slot_map;
-    // slot_tab[s] is the number of unique splitters whose slot is below s, so
-    // the splitters that a key of slot s still has to be compared with are
-    // uniq[slot_tab[s] .. slot_tab[s+1]).
+    // [slot_map.lo, slot_hi] and mapped to SPLIT_SLOTS slots by slot_map.
+    // Entry s packs lo | cnt << 8: lo = the number of unique splitters whose
+    // slot is below s, cnt = how many share slot s.  A key of slot s has lo
+    // splitters below it for sure and still has to be compared with
+    // uniq[lo .. lo+cnt) -- none for most keys (255 splitters, 4096 slots).
     SlotMap<K> slot_map;
     K slot_hi;
-    alignas(16) uint8_t slot_tab[SPLIT_SLOTS + 4];
+    alignas(16) uint16_t slot_tab[SPLIT_SLOTS + 8];
 };
 
 // A bucket that a leaf kernel sorts (or copies) into its final place.
@@ -144,6 +142,7 @@ struct LevelCtl {
     uint32_t learned_used;    // segments routed by their learned model
     uint32_t plain_used;      // segments routed by the splitter tree
     uint32_t n_uneven[NCLASS];  // leaves handed from the slot sort to the block sort
+    uint32_t never_set;       // testing: a flag nothing writes (the injected wait)
     double bucket_sq;         // sum of squared non-empty bucket sizes this level
 };
 
@@ -258,13 +257,18 @@ __global__ void __launch_bounds__(256) splitter_kernel(const K* __restrict__ sam
             out->slot_hi = smp[m - 1];
         }
         __syncthreads();
-        for (uint32_t s = t; s < (uint32_t)SPLIT_SLOTS + 4; s += NB) {
-            uint32_t lo = 0, hi = K_u;  // splitters with slot < s
+        auto below = [&](uint32_t s) {  // splitters with slot < s
+            uint32_t lo = 0, hi = K_u;
             while (lo < hi) {
                 const uint32_t mid = (lo + hi) >> 1;
                 if (sk[mid] < s) lo = mid + 1; else hi = mid;
             }
-            out->slot_tab[s] = (uint8_t)lo;
+            return lo;
+        };
+        for (uint32_t s = t; s < (uint32_t)SPLIT_SLOTS + 8; s += NB) {
+            const uint32_t lo = below(s);
+            const uint32_t cnt = s < (uint32_t)SPLIT_SLOTS ? below(s + 1) - lo : 0u;
+            out->slot_tab[s] = (uint16_t)(lo | (cnt << 8));
         }
     }
     // bucket ids: range_j, then eq_j if splitter j has one; the last range bucket is K_u
@@ -351,26 +355,28 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
 }
 
 // The same bucket through the splitter lookup table: the key's slot gives the
-// unique splitters below it up to the few that share its slot, which a binary
-// search over uniq[] settles (slot_tab is monotone, so tab[s] <= tab[s+1]).
+// unique splitters below it and the few that share its slot, which are
+// settled by comparisons with uniq[] (none for most keys).
 template <typename K>
-__device__ __forceinline__ uint32_t find_bucket_tab(const uint8_t* __restrict__ tab, const SlotMap<K>& f, K fhi,
+__device__ __forceinline__ uint32_t find_bucket_tab(const uint16_t* __restrict__ tab, const SlotMap<K>& f, K fhi,
                                                     K x, bool has_eq, const K* __restrict__ uniq,
                                                     const uint8_t* __restrict__ range_b,
                                                     const uint8_t* __restrict__ eq_b,
                                                     const uint32_t* __restrict__ eq_mask) {
     const K xc = kmin(kmax(x, f.lo), fhi);
-    const uint32_t s = f(xc);
-    uint32_t lo = tab[s], hi = tab[s + 1];
-    if (hi - lo == 1) {  // the common case: one splitter shares the key's slot
+    const uint32_t e = tab[f(xc)];
+    uint32_t lo = e & 0xFFu;
+    const uint32_t cnt = e >> 8;
+    if (cnt == 1) {  // one splitter shares the key's slot
         lo += uniq[lo] < x ? 1u : 0u;
-    } else {
+    } else if (cnt > 1) {
+        uint32_t hi = lo + cnt;
         while (lo < hi) {
             const uint32_t mid = (lo + hi) >> 1;
             if (uniq[mid] < x) lo = mid + 1; else hi = mid;
         }
     }
-    const uint32_t j = lo;
+    const uint32_t j = lo;  // number of unique splitters < x
     if (!has_eq) return j;
     if (j < 255 && ((eq_mask[j >> 5] >> (j & 31)) & 1u) && uniq[j] == x) return eq_b[j];
     return range_b[j];
@@ -383,28 +389,33 @@ __device__ __forceinline__ uint32_t find_bucket_tab(const uint8_t* __restrict__ 
 namespace s512 {
 
 // ===========================================================================
-// 4. The partition pass (persistent; tiles claimed in order)
+// 4. The partition pass (persistent; tiles claimed in runs)
 //
-// Two-stage pipeline per block: while tile i is classified, ranked and
-// scattered, tile i+1 is already on its way into the other shared-memory
-// buffer through a 1-D bulk copy (TMA) that completes on an mbarrier.  Data
-// tiles are claimed two ahead with an atomic counter.  The position of a tile
-// in its segment's look-back chain is taken separately, from a per-segment
-// counter, when the block *starts* processing it: every earlier position then
-// belongs to a tile already being processed, so no tile waits for one that is
-// still only being fetched.  (A bucket's keys land in chain order, not input
-// order; a partition pass does not need to be stable.)  The buffer that held
-// tile i's raw keys is reused to stage its keys in bucket order for the
-// coalesced write.  When an input array is not 16-byte aligned the tiles are
+// Every tile of keys is classified, ranked within the tile by shared-memory
+// atomics, staged in bucket order in shared memory and written out with
+// coalesced stores.  Where a tile's keys of bucket b go inside the bucket's
+// region is reserved with one global atomic add per (tile, bucket) on the
+// segment's fill counter of b: the pass is not stable (a bucket's keys land in
+// the order their tiles reserved, and the leaves sort them anyway), so no
+// tile ever waits for another and tiles may be processed in any order.  The
+// counters end as the bucket sizes.  A reservation past the region's
+// capacity (the sample's 6-sigma bound) drops the tile's keys of that bucket
+// and reports an overflow; the level is then redone with exact counts.
+//
+// Pipeline per block: the next tile travels into the second shared-memory
+// buffer by a 1-D bulk copy (TMA, completing on an mbarrier) while the
+// current one is ranked, staged and written; the buffer that held a tile's
+// raw keys is reused to stage them in bucket order.  Three block barriers per
+// tile: histogram complete | bucket starts known | staging complete.  Two
+// blocks share an SM, so one block's barrier phases overlap the other's
+// memory traffic.  When an input array is not 16-byte aligned the tiles are
 // read with plain loads instead (a.tma == 0).
-
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
 // Consecutive tiles a block claims at once: one segment's tables are loaded
 // once per group, so levels with many segments take longer runs; a single
 // segment takes short ones (a finer split of the last tiles among blocks).
 constexpr uint32_t CLAIM_GROUP_ONE_SEG = 4;
 constexpr uint32_t CLAIM_GROUP_MANY_SEGS = 16;
-constexpr int LOOKBACK_W = 2;  // predecessor statuses read per look-back step
 constexpr uint64_t GDELTA_DROP = ~0ull;  // write offset of a bucket that overflowed its region
 
 template <typename K>
@@ -414,16 +425,15 @@ struct PartArgs {
     const uint32_t* tile_seg;     // global tile -> segment (nullptr: single segment 0)
     const SplitSet<K>* splits;
     K* out;                       // level output buffer
-    unsigned long long* status;   // ntiles * NB
-    uint64_t* bucket_counts;      // nsegs * NB, written by each segment's last tile
+    unsigned long long* fill;     // nsegs * NB fill counters (zeroed); end as the bucket sizes
     LevelCtl* ctl;
-    uint32_t ntiles;              // used when ntiles_dev is null
+    uint32_t ntiles;              // end of the launch's tiles (used when ntiles_dev is null)
     const uint32_t* ntiles_dev;   // tile count written by prepare_level_kernel
+    uint32_t tile_first;          // first tile of the launch (a level fed in chunks launches per chunk)
+    uint32_t* tile_counter;       // the launch's claim counter (zeroed)
     int tma;                      // tiles arrive by bulk copy
-    uint32_t* chain;              // per segment: look-back positions handed out so far (zeroed)
     const LearnedSet<K>* learned; // per segment learned model (nullptr: splitters only)
-    uint32_t inject_slot;         // testing: chain position 1 of segment 0 waits on this
-                                  // never-written status slot (0xFFFFFFFF: off)
+    int inject_timeout;           // testing: tile 1 waits, with a short bound, on a flag nothing sets
 };
 
 // The routing tables of a plain split set, as the partition pass keeps them.
@@ -435,7 +445,7 @@ struct PlainTables {
     uint32_t eq_mask[NB / 32];
     SlotMap<K> fmap;
     K fhi;
-    alignas(16) uint8_t tab[SPLIT_SLOTS + 4];
+    alignas(16) uint16_t tab[SPLIT_SLOTS + 8];
 };
 
 // Bytes of a LearnedSet that inference reads (its leading fields).
@@ -453,9 +463,8 @@ struct PartSmem {
     uint32_t hist[NB];
     uint32_t loc[NB];
     uint32_t seg_tile_start[SEG_SMEM];
-    uint32_t wtot[8];
     uint64_t mbar[2];
-    uint32_t tile_cur, tile_next, has_eq, nbk, abort, pos, use_learned;
+    uint32_t tile_cur, has_eq, use_learned, abort;
     SegDesc sd;                   // segment of the tile being processed
     SegDesc iss_sd;               // thread 0: segment of the last tile it fetched
     uint32_t iss_seg;
@@ -474,6 +483,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
     constexpr int TILE = THREADS * IPT;
     constexpr int ESZ = InCodec::ESZ;
     constexpr int NARR = InCodec::NARR;
+    static_assert(TILE < (1 << 24), "rank and bucket share a 32-bit word");
     const int tid = threadIdx.x;
     const uint32_t ntiles = a.ntiles_dev ? *a.ntiles_dev : a.ntiles;
     const bool small_tab = a.tile_seg && a.nsegs <= (uint32_t)SEG_SMEM;
@@ -524,45 +534,38 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
         }
     };
 
-    uint32_t claim_after = 0;  // thread 0: the tile claimed for two iterations ahead
-    const uint32_t claim_group = a.nsegs > 1 ? CLAIM_GROUP_MANY_SEGS : CLAIM_GROUP_ONE_SEG;
     // thread 0 claims claim_group consecutive tiles at a time, so that a block
     // works through a run of one segment before it loads another's tables
+    const uint32_t claim_group = a.nsegs > 1 ? CLAIM_GROUP_MANY_SEGS : CLAIM_GROUP_ONE_SEG;
     uint32_t grp_next = 0, grp_end = 0;
     auto claim = [&]() -> uint32_t {
         if (grp_next == grp_end) {
-            grp_next = atomicAdd(&a.ctl->tile_counter, claim_group);
+            grp_next = a.tile_first + atomicAdd(a.tile_counter, claim_group);
             grp_end = grp_next + claim_group;
         }
         return grp_next++;
     };
+    uint32_t t_next = 0;  // thread 0: the tile after the current one
     if (tid == 0) {
         const uint32_t t0 = claim();
-        const uint32_t t1 = claim();
         sm.tile_cur = t0;
-        sm.tile_next = t1;
         if (a.tma && t0 < ntiles) issue(t0, 0);
+        t_next = claim();
     }
     __syncthreads();
-    uint32_t phase[2] = {0u, 0u};
+    uint32_t phases = 0;  // bit b: the parity to wait for on buffer b's mbarrier
     int b = 0;
 
     while (true) {
-        // tile_cur / tile_next are rewritten by thread 0 only after the
-        // barriers below, so reading them needs no barrier of its own
+        // tile_cur is rewritten by thread 0 only after the first barrier of
+        // the iteration, and read again after the last one
         const uint32_t t = sm.tile_cur;
-        const uint32_t tn = sm.tile_next;
         if (t >= ntiles || sm.abort) break;
         const uint32_t seg = seg_of(t);
-        uint32_t my_pos = 0;  // thread 0: look-back position of tile t (stored before the rank barrier)
-        if (tid == 0) {
-            if (a.tma && tn < ntiles) issue(tn, b ^ 1);
-            claim_after = claim();  // consumed at the end of the iteration
-            my_pos = atomicAdd(&a.chain[seg], 1u);
-        }
         const bool new_seg = seg != cached_seg;
         if (new_seg) {
-            // the segment's descriptor and tables, read once per run of its tiles
+            // the segment's descriptor and tables, read once per run of its
+            // tiles (the previous tile's write-out reads none of them)
             if (tid < (int)(sizeof(SegDesc) / 4))
                 reinterpret_cast<uint32_t*>(&sm.sd)[tid] = reinterpret_cast<const uint32_t*>(&a.segs[seg])[tid];
             const bool use_learned = a.learned && a.learned[seg].ok;
@@ -575,7 +578,6 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                     sm.region_off[i] = ls.region_off[i];
                     sm.region_cap[i] = ls.region_cap[i];
                 }
-                if (tid == 0) sm.nbk = ls.nbuckets;
             } else {
                 const SplitSet<K>& ss = a.splits[seg];
                 for (int i = tid; i < NB; i += THREADS) {
@@ -587,13 +589,12 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 }
                 if (tid < NB / 32) sm.T.P.eq_mask[tid] = ss.eq_mask[tid];
                 {
-                    const uint32_t* src = reinterpret_cast<const uint32_t*>(ss.slot_tab);
-                    uint32_t* dst = reinterpret_cast<uint32_t*>(sm.T.P.tab);
-                    for (int i = tid; i < (SPLIT_SLOTS + 4) / 4; i += THREADS) dst[i] = src[i];
+                    const uint4* src = reinterpret_cast<const uint4*>(ss.slot_tab);
+                    uint4* dst = reinterpret_cast<uint4*>(sm.T.P.tab);
+                    for (int i = tid; i < (SPLIT_SLOTS + 8) * 2 / 16; i += THREADS) dst[i] = src[i];
                 }
                 if (tid == 0) {
                     sm.has_eq = ss.has_eq;
-                    sm.nbk = ss.nbuckets;
                     sm.T.P.fmap = ss.slot_map;
                     sm.T.P.fhi = ss.slot_hi;
                 }
@@ -605,22 +606,31 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
         if (a.tma) {
             // every thread waits on the barrier itself: the bulk copy's data is
             // then visible to it without a block barrier
-            data_ok = mbar_wait_bounded(&sm.mbar[b], phase[b]);
-            phase[b] ^= 1u;
+            data_ok = mbar_wait_bounded(&sm.mbar[b], (phases >> b) & 1u);
+            phases ^= 1u << b;
             if (!data_ok) raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
         }
+        if (a.inject_timeout && t == 1) {
+            // injected failure: a wait on a flag that nothing sets, with a
+            // short bound; the tile then gives up and writes nothing
+            uint32_t spins = 0;
+            while (!*(volatile uint32_t*)&a.ctl->never_set && ++spins < 1024u) __nanosleep(100);
+            data_ok = false;
+            raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
+        }
         if (new_seg) __syncthreads();  // the segment's descriptor and tables in shared memory
-        const SegDesc sd = sm.sd;
-        const uint32_t ti = t - sd.tile_start;
-        const uint64_t base = sd.in_off + (uint64_t)ti * TILE;
-        const uint64_t rem = sd.count - (uint64_t)ti * TILE;
+        // (the descriptor stays in shared memory: registers hold the keys)
+        const uint32_t ti = t - sm.sd.tile_start;
+        const uint64_t base = sm.sd.in_off + (uint64_t)ti * TILE;
+        const uint64_t rem = sm.sd.count - (uint64_t)ti * TILE;
         const uint32_t cnt = rem < (uint64_t)TILE ? (uint32_t)rem : (uint32_t)TILE;
         const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
         const bool has_eq = sm.has_eq != 0;
         const bool learned = sm.use_learned != 0;
 
-        // keys: striped element r*THREADS + tid, from the bulk-copied tile
-        // (tail elements past the copied bytes from global memory)
+        // A. keys (striped: element r*THREADS + tid, from the bulk-copied
+        // tile; tail elements past the copied bytes from global memory),
+        // their buckets and their ranks within the tile
         K key[IPT];
         uint32_t br[IPT];  // bucket | rank << 8
 #pragma unroll
@@ -663,19 +673,16 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
             }
             br[r] = bk | (rank << 8);
         }
-        if (tid == 0) sm.pos = my_pos;
-        __syncthreads();
+        __syncthreads();  // (1) the tile's histogram is complete; the previous tile is written
 
-        // publish this tile's aggregate (or its inclusive count if first in chain)
-        const uint32_t pos = sm.pos;
-        const uint32_t slot = sd.tile_start + pos;
+        // B. reserve the tile's share of each bucket's region, and the
+        // buckets' starts within the tile (exclusive scan by warp 0)
         uint32_t h = 0;
+        unsigned long long off = 0;
         if (tid < NB) {
             h = sm.hist[tid];
-            const unsigned long long w = (pos == 0 ? ST_INC : ST_AGG) | (unsigned long long)h;
-            st_status(&a.status[(size_t)slot * NB + tid], w);
+            if (h) off = atomicAdd(&a.fill[(size_t)seg * NB + tid], (unsigned long long)h);
         }
-        // exclusive scan of the 256 bucket counts by warp 0 (8 per lane)
         if (tid < 32) {
             uint32_t v[NB / 32];
             uint32_t run = 0;
@@ -694,9 +701,16 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
 #pragma unroll
             for (int i = 0; i < NB / 32; ++i) sm.loc[tid * (NB / 32) + i] = ex + v[i];
         }
-        __syncthreads();
+        if (tid == 0) {
+            // the next tile's keys into the other buffer: its last reader, the
+            // previous tile's write-out, finished before barrier (1)
+            if (a.tma && t_next < ntiles) issue(t_next, b ^ 1);
+            sm.tile_cur = t_next;
+            t_next = claim();
+        }
+        __syncthreads();  // (2) bucket starts within the tile
 
-        // stage keys in bucket order, reusing this tile's buffer
+        // C. stage the keys in bucket order, reusing this tile's buffer
         K* stage = reinterpret_cast<K*>(sm.buf[b]);
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
@@ -708,64 +722,17 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 sm.bkt[p] = (uint8_t)bk;
             }
         }
-
-        // decoupled look-back: one thread per bucket
         if (tid < NB) {
-            uint64_t prefix = 0;
-            bool ok = data_ok;
-            if (pos == 1 && seg == 0 && a.inject_slot != 0xFFFFFFFFu) {
-                // injected failure: a predecessor that never publishes, waited
-                // for with a short bound
-                uint32_t spins = 0;
-                while (!(ld_status(&a.status[(size_t)a.inject_slot * NB + tid]) & (ST_INC | ST_AGG)) &&
-                       ++spins < 1024u)
-                    __nanosleep(100);
-                ok = false;
-                raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
-                st_status(&a.status[(size_t)slot * NB + tid], ST_INC | (unsigned long long)h);
-            } else if (pos > 0) {
-                // walk back through the chain LOOKBACK_W slots at a time (the
-                // loads of one window are in flight together); the segment's
-                // first slot always holds an inclusive count, so the walk ends
-                constexpr int W = LOOKBACK_W;
-                int64_t p = (int64_t)slot - 1;
-                const int64_t first = (int64_t)sd.tile_start;
-                bool done = false;
-                while (!done && ok) {
-                    unsigned long long v[W];
-#pragma unroll
-                    for (int w = 0; w < W; ++w)
-                        v[w] = (p - w >= first) ? ld_status(&a.status[(size_t)(p - w) * NB + tid]) : 0ull;
-#pragma unroll
-                    for (int w = 0; w < W; ++w) {
-                        if (done || !ok || p - w < first) continue;
-                        uint32_t spins = 0;
-                        while (!(v[w] & (ST_INC | ST_AGG))) {
-                            if (++spins > SPIN_LIMIT) break;
-                            __nanosleep(spins < 64 ? 20 : 200);
-                            v[w] = ld_status(&a.status[(size_t)(p - w) * NB + tid]);
-                        }
-                        if (!(v[w] & (ST_INC | ST_AGG))) {
-                            ok = false;
-                            raise_error(&a.ctl->err, DEV_ERR_TIMEOUT);
-                            continue;
-                        }
-                        prefix += v[w] & ST_VAL;
-                        if (v[w] & ST_INC) done = true;
-                    }
-                    p -= W;
-                }
-                st_status(&a.status[(size_t)slot * NB + tid], ST_INC | (unsigned long long)(prefix + h));
-            }
-            const uint64_t end = prefix + h;
-            const bool ovf = !ok || end > sm.region_cap[tid];
-            if (ovf && h) raise_error(&a.ctl->err, ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
-            sm.gdelta[tid] = ovf ? GDELTA_DROP : sd.out_base + sm.region_off[tid] + prefix - (uint64_t)sm.loc[tid];
-            if (pos == sd.ntiles - 1) a.bucket_counts[(size_t)seg * NB + tid] = end;
+            const unsigned long long end = off + h;
+            const bool ovf = !data_ok || end > sm.region_cap[tid];
+            if (ovf && h) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
+            sm.gdelta[tid] = ovf ? GDELTA_DROP : sm.sd.out_base + sm.region_off[tid] + off - (uint64_t)sm.loc[tid];
+            sm.hist[tid] = 0;  // (next used after barrier (3))
         }
-        __syncthreads();
+        if (tid == 0 && !data_ok) sm.abort = 1;
+        __syncthreads();  // (3) staging complete
 
-        // coalesced write-out (an overflowed bucket's keys are dropped: the
+        // D. coalesced write-out (an overflowed bucket's keys are dropped: the
         // level is redone)
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
@@ -775,17 +742,10 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 if (g != GDELTA_DROP) a.out[g + i] = stage[i];
             }
         }
-        if (tid < NB) sm.hist[tid] = 0;
-        if (tid == 0) {
-            sm.tile_cur = tn;
-            sm.tile_next = claim_after;
-            if (!data_ok) sm.abort = 1;
-        }
-        __syncthreads();
         b ^= 1;
     }
     // after an abort, let a copy still in flight land before the block exits
-    if (a.tma && sm.abort && tid == 0 && sm.tile_cur < ntiles) mbar_wait_bounded(&sm.mbar[b], phase[b]);
+    if (a.tma && sm.abort && tid == 0 && sm.tile_cur < ntiles) mbar_wait_bounded(&sm.mbar[b], (phases >> b) & 1u);
 }
 
 // Testing: shrink every bucket capacity of segment 0 (forces an overflow).
@@ -839,8 +799,7 @@ __global__ void __launch_bounds__(THREADS) count_kernel(PartArgs<K> a, InCodec i
         }
         __syncthreads();
         for (int b = threadIdx.x; b < NB; b += THREADS)
-            if (hist[b]) atomicAdd((unsigned long long*)&a.bucket_counts[(size_t)seg * NB + b],
-                                   (unsigned long long)hist[b]);
+            if (hist[b]) atomicAdd(&a.fill[(size_t)seg * NB + b], (unsigned long long)hist[b]);
         __syncthreads();
     }
 }

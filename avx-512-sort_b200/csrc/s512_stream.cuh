@@ -72,7 +72,12 @@ inline size_t stream_piece_keys(size_t esz) {
     return m < 65536 ? 65536 : m;
 }
 
-inline bool stream_needed(size_t n, size_t esz) { return n > stream_piece_keys(esz); }
+// Whether a host array must be streamed.  Without a configured budget, a
+// working set under 1 GiB never is (no free-memory query on small calls).
+inline bool stream_needed(size_t n, size_t esz) {
+    if (!config().device_budget && n * esz * 6 < ((size_t)1 << 30)) return false;
+    return n > stream_piece_keys(esz);
+}
 
 // Number of keys of the sorted run r[0..len) whose encoded key is <= v (or < v).
 template <typename T>

@@ -5,13 +5,18 @@
  * Plain pointers and sizes only.  Every function returns an int status
  * (S512_OK == 0).  Pointers may be host or device memory: with S512_PTR_AUTO
  * (the default) the library asks the CUDA driver which one it is; host data is
- * copied to the device, sorted there and copied back before the call returns.
- * Device data is sorted in place on `stream` (a cudaStream_t, NULL = the
- * default stream); the call waits for the result unless S512_ASYNC is set.
+ * copied to the device, sorted there and copied back.  Device data is sorted
+ * in place on `stream` (a cudaStream_t, NULL = the default stream).  A call
+ * waits for its result unless S512_ASYNC is set; with S512_ASYNC, device data
+ * and page-locked host data (cudaHostAlloc / cudaHostRegister) are ready once
+ * the stream has finished, pageable host data is always waited for.  A sort
+ * of large page-locked host arrays copies them in by chunks on a second
+ * stream and starts partitioning each chunk as it lands.
  *
  * Every operation is in place, like the reference.  Scratch memory comes from
- * a per-device pool that grows on demand and is kept until
- * s512_release_scratch() or process exit.
+ * one pool per (device, stream) that grows on demand and is kept until
+ * s512_release_scratch() or process exit; calls on different streams use
+ * different pools, so they may overlap on the device.
  *
  * Element types: int32 ("i32"), double ("f64") and int32 key + int32 value
  * pairs held in two arrays ("kv_i32").  Results:
@@ -44,7 +49,7 @@ enum {
     S512_OK = 0,
     S512_ERR_ARG = 1,         /* bad argument (null pointer with n > 0, left > right, ...) */
     S512_ERR_ALLOC = 2,       /* device or pinned allocation failed */
-    S512_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up (look-back spin) */
+    S512_ERR_TIMEOUT = 3,     /* a bounded device-side wait gave up (look-back spin, bulk copy) */
     S512_ERR_CUDA = 4,        /* a CUDA runtime call failed; see s512_last_error_string() */
     S512_ERR_INTERNAL = 5,    /* an internal capacity check failed */
     S512_ERR_UNSUPPORTED = 6  /* no usable sm_100 device */
@@ -58,7 +63,7 @@ enum {
     S512_SPLIT_AUTO = 0,      /* splitter mode from s512_config (default: plain) */
     S512_SPLIT_PLAIN = 4,     /* sampled splitters + binary search */
     S512_SPLIT_LEARNED = 8,   /* learned monotone CDF model, plain splitters as fallback */
-    S512_ASYNC = 16           /* device pointers: return without waiting for the stream */
+    S512_ASYNC = 16           /* device or page-locked host data: return without waiting for the stream */
 };
 
 /* library configuration (process wide) */
@@ -77,9 +82,9 @@ typedef struct s512_config {
  * OVERFLOW shrinks the first level's bucket capacities so the partition pass
  * overflows and the level is redone with exact counts; REJECT_MODEL rejects
  * every learned model so the splitters route every level; ALLOC makes scratch
- * allocation fail; TIMEOUT makes one tile of the first level wait on a status
- * word that is never written, with a short bound, so the call returns
- * S512_ERR_TIMEOUT while the device stays usable. */
+ * allocation fail; TIMEOUT makes one tile of the first partition level (or of
+ * Partition512) wait on a device flag that is never set, with a short bound,
+ * so the call returns S512_ERR_TIMEOUT while the device stays usable. */
 enum {
     S512_FAULT_OVERFLOW = 1,
     S512_FAULT_REJECT_MODEL = 2,
