@@ -4,9 +4,9 @@
 // A batch is many independent arrays stored back to back (segment s is
 // data[offsets[s], offsets[s+1])).  The reference sorts such a batch with a
 // loop of SmallSort16V / Sort calls (sort512perf.cpp:612-709 timeSmall).
-// Here: one classification kernel, one persistent launch for every segment
-// that fits a block (segsort_small_kernel), and the partition levels for the
-// few longer segments, all on one stream.
+// Here: one classification kernel, one persistent launch for the warp-sized
+// segments and one per block size class (1K..16K keys) that has segments,
+// and the partition levels for the few longer segments, all on one stream.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -18,13 +18,11 @@
 namespace s512 {
 
 // ---------------------------------------------------------------------------
-// launch shapes of the persistent kernel (the autotuner's search space)
-struct SegShape {
-    int threads, ept;
-};
-static const SegShape kSegShapes[] = {{256, 16}, {512, 8}, {512, 16}, {1024, 8}};
+// The autotuner's search space: the largest block class used (segments above
+// it run the partition levels).  Shape i uses classes 0..kSegShapeTop[i].
+static const int kSegShapeTop[] = {1, 2, 3, 4};
 constexpr int kNumSegShapes = 4;
-constexpr int kDefaultSegShape = 2;  // 512 x 16: blocks of up to 8192 keys
+constexpr int kDefaultSegShape = 3;  // blocks of up to 16384 keys
 
 enum { DT_I32 = 0, DT_F64 = 1, DT_KV = 2, NUM_DT = 3 };
 static int g_seg_shape[NUM_DT] = {-1, -1, -1};
@@ -80,60 +78,92 @@ static int seg_shape_for(int dt) {
     return g_seg_shape[dt] >= 0 ? g_seg_shape[dt] : kDefaultSegShape;
 }
 
-// ---------------------------------------------------------------------------
-// prepare_only: set the kernel's attributes and size its grid without
-// launching (done before a stream capture, where those calls do not belong)
-template <typename Codec, int T, int E>
-static int launch_small(DevCtx& C, Codec io, const SegItem* wi, const SegItem* bi, SegCtl* ctl, cudaStream_t st,
-                        bool prepare_only) {
-    using K = typename Codec::Key;
-    auto fn = segsort_small_kernel<Codec, T, E>;
-    const size_t block_bytes = SlotSmem<K, T, E>::bytes;
-    const size_t warp_bytes = (size_t)(T / 32) * WARP_REGION * sizeof(K);
-    const size_t smem = block_bytes > warp_bytes ? block_bytes : warp_bytes;
-    int grid = 0;
-    S512_CUDA_TRY(launch_persistent(C, fn, T, smem, st, 0, &grid));
-    if (prepare_only) return S512_OK;
-    fn<<<grid, T, smem, st>>>(io, wi, bi, ctl);
-    S512_LAUNCH_CHECK();
-    return S512_OK;
-}
-
-template <typename Codec>
-static int launch_small_shape(DevCtx& C, int shape, Codec io, const SegItem* wi, const SegItem* bi, SegCtl* ctl,
-                              cudaStream_t st, bool prepare_only = false) {
-    switch (shape) {
-        case 0: return launch_small<Codec, 256, 16>(C, io, wi, bi, ctl, st, prepare_only);
-        case 1: return launch_small<Codec, 512, 8>(C, io, wi, bi, ctl, st, prepare_only);
-        case 2: return launch_small<Codec, 512, 16>(C, io, wi, bi, ctl, st, prepare_only);
-        default: return launch_small<Codec, 1024, 8>(C, io, wi, bi, ctl, st, prepare_only);
-    }
-}
-
-static uint32_t shape_cap(int shape) { return (uint32_t)(kSegShapes[shape].threads * kSegShapes[shape].ept); }
+static uint32_t shape_cap(int shape) { return seg_class_cap(kSegShapeTop[shape]); }
 
 // Work lists of one batch (device memory).
 struct SegLists {
     SegItem* warp_items = nullptr;
-    SegItem* block_items = nullptr;
+    SegItem* cls_items = nullptr;  // SEG_NCLASS lists of stride nseg + 1
+    size_t stride = 0;
     SegDesc* big = nullptr;
     SegCtl* ctl = nullptr;
 };
 
 static int seg_lists_pool(DevCtx& C, size_t nseg, SegLists* L) {
+    L->stride = nseg + 1;
     L->warp_items = (SegItem*)C.get("seg_warp", (nseg + 1) * sizeof(SegItem));
-    L->block_items = (SegItem*)C.get("seg_block", (nseg + 1) * sizeof(SegItem));
+    L->cls_items = (SegItem*)C.get("seg_block", SEG_NCLASS * (nseg + 1) * sizeof(SegItem));
     L->big = (SegDesc*)C.get("seg_big", (nseg + 1) * sizeof(SegDesc));
     L->ctl = (SegCtl*)C.get("seg_ctl", sizeof(SegCtl));
-    return (L->warp_items && L->block_items && L->big && L->ctl) ? S512_OK : S512_ERR_ALLOC;
+    return (L->warp_items && L->cls_items && L->big && L->ctl) ? S512_OK : S512_ERR_ALLOC;
 }
 
 static int classify(const size_t* d_off, size_t nseg, uint32_t cap, const SegLists& L, cudaStream_t st) {
     S512_CUDA_TRY(cudaMemsetAsync(L.ctl, 0, sizeof(SegCtl), st));
     const int grid = (int)std::min<size_t>((nseg + 255) / 256, 4096);
-    segsort_classify_kernel<<<grid > 0 ? grid : 1, 256, 0, st>>>(d_off, nseg, cap, L.warp_items, L.block_items,
-                                                                  L.big, L.ctl);
+    segsort_classify_kernel<<<grid > 0 ? grid : 1, 256, 0, st>>>(d_off, nseg, cap, L.warp_items, L.cls_items,
+                                                                  L.stride, L.big, L.ctl);
     S512_LAUNCH_CHECK();
+    return S512_OK;
+}
+
+// prepare_only: set the kernel's attributes without launching (done before a
+// stream capture, where those calls do not belong).  n: the class's segment
+// count (the grid is no larger).
+template <typename Codec, int T, int E>
+static int launch_block_class(DevCtx& C, Codec io, const SegItem* items, const uint32_t* d_n, uint32_t n,
+                              cudaStream_t st, bool prepare_only) {
+    using K = typename Codec::Key;
+    auto fn = segsort_block_kernel<Codec, T, E>;
+    const size_t smem = SlotSmem<K, T, E>::bytes;
+    int grid = 0;
+    S512_CUDA_TRY(launch_persistent(C, fn, T, smem, st, (int)n, &grid));
+    if (prepare_only || n == 0) return S512_OK;
+    fn<<<grid, T, smem, st>>>(io, items, d_n);
+    S512_LAUNCH_CHECK();
+    return S512_OK;
+}
+
+// Every segment of up to the shape's largest class, given the class counts
+// read back after classification.
+template <typename Codec>
+static int launch_classes(DevCtx& C, int shape, Codec io, const SegLists& L, const SegCtl& h, cudaStream_t st,
+                          uint32_t* launches, bool prepare_only = false) {
+    {
+        auto fn = segsort_warp_kernel<Codec>;
+        int grid = 0;
+        S512_CUDA_TRY(launch_persistent(C, fn, 256, 0, st, (int)((h.n_warp + 7) / 8), &grid));
+        if (!prepare_only && h.n_warp) {
+            fn<<<grid, 256, 0, st>>>(io, L.warp_items, L.ctl);
+            S512_LAUNCH_CHECK();
+            ++*launches;
+        }
+    }
+    const int top = kSegShapeTop[shape];
+    for (int c = top; c >= 0; --c) {  // the longest segments first
+        const SegItem* items = L.cls_items + (size_t)c * L.stride;
+        const uint32_t* d_n = &L.ctl->n_cls[c];
+        const uint32_t n = h.n_cls[c];
+        // 8 keys per thread where a class allows it: 64-bit keys with 16 per
+        // thread (plus the inline block sort) run out of registers
+        constexpr bool wide = sizeof(typename Codec::Key) == 8;
+        int rc;
+        switch (c) {
+            case 0: rc = launch_block_class<Codec, 128, 8>(C, io, items, d_n, n, st, prepare_only); break;
+            case 1: rc = launch_block_class<Codec, 256, 8>(C, io, items, d_n, n, st, prepare_only); break;
+            case 2:
+                rc = wide ? launch_block_class<Codec, 512, 8>(C, io, items, d_n, n, st, prepare_only)
+                          : launch_block_class<Codec, 256, 16>(C, io, items, d_n, n, st, prepare_only);
+                break;
+            case 3:
+                rc = wide ? launch_block_class<Codec, 1024, 8>(C, io, items, d_n, n, st, prepare_only)
+                          : launch_block_class<Codec, 512, 16>(C, io, items, d_n, n, st, prepare_only);
+                break;
+            default: rc = launch_block_class<Codec, 1024, 16>(C, io, items, d_n, n, st, prepare_only); break;
+        }
+        if (rc) return rc;
+        if (!prepare_only && n) ++*launches;
+    }
     return S512_OK;
 }
 
@@ -145,7 +175,7 @@ static int sort_big(DevCtx& C, Codec io, const SegLists& L, uint32_t n_big, uint
     return run_levels<K, Codec, Codec>(C, io, io, L.big, n_big, big_keys, st, tm, S, false);
 }
 
-// The whole batch on the device: classify, persistent launch, long segments.
+// The whole batch on the device: classify, the class launches, long segments.
 template <typename K, typename Codec>
 static int segsort_device(DevCtx& C, Codec io, const size_t* d_off, size_t nseg, int dt, cudaStream_t st) {
     s512_stats& S = thread_stats();
@@ -159,17 +189,16 @@ static int segsort_device(DevCtx& C, Codec io, const size_t* d_off, size_t nseg,
     const int shape = seg_shape_for(dt);
     rc = classify(d_off, nseg, shape_cap(shape), L, st);
     if (rc) return rc;
-    rc = launch_small_shape<Codec>(C, shape, io, L.warp_items, L.block_items, L.ctl, st);
-    if (rc) return rc;
-    S.kernel_launches += 2;
     SegCtl* h = (SegCtl*)C.host_pinned(sizeof(SegCtl));
     if (!h) return S512_ERR_ALLOC;
     S512_CUDA_TRY(cudaMemcpyAsync(h, L.ctl, sizeof(SegCtl), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaStreamSynchronize(st));
-    const uint32_t n_big = h->n_big;
-    const uint64_t big_keys = h->big_keys;
+    const SegCtl counts = *h;
+    S.kernel_launches += 1;
+    rc = launch_classes<Codec>(C, shape, io, L, counts, st, &S.kernel_launches);
+    if (rc) return rc;
     const int t1 = tm.mark();
-    rc = sort_big<K, Codec>(C, io, L, n_big, big_keys, st, tm, S);
+    rc = sort_big<K, Codec>(C, io, L, counts.n_big, counts.big_keys, st, tm, S);
     if (rc) return rc;
     const int t2 = tm.mark();
     if (tm.on()) {
@@ -258,11 +287,14 @@ static int tune_dtype(DevCtx& C, int dt, Codec io, uint64_t total, const size_t*
             segsort_fill_kernel<Codec><<<1024, 256, 0, st>>>(io, total, 0x7u + (uint64_t)rep);
             cudaEventRecord(e0, st);
             rc = classify(d_off, nseg, shape_cap(shape), L, st);
-            if (!rc) rc = launch_small_shape<Codec>(C, shape, io, L.warp_items, L.block_items, L.ctl, st);
             SegCtl h;
             if (!rc) {
                 cudaMemcpyAsync(&h, L.ctl, sizeof(SegCtl), cudaMemcpyDeviceToHost, st);
                 cudaStreamSynchronize(st);
+                uint32_t launches = 0;
+                rc = launch_classes<Codec>(C, shape, io, L, h, st, &launches);
+            }
+            if (!rc) {
                 PhaseTimer tm(st, false);
                 s512_stats S;
                 memset(&S, 0, sizeof(S));
@@ -294,8 +326,8 @@ static int tune_dtype(DevCtx& C, int dt, Codec io, uint64_t total, const size_t*
 }
 
 // ---------------------------------------------------------------------------
-// graph plan: the classification is done once; the persistent launch (and the
-// reset of its queue counters) is captured in a CUDA graph and replayed
+// graph plan: the classification is done once; the class launches are
+// captured in a CUDA graph and replayed
 
 struct Plan {
     int dt;
@@ -304,14 +336,24 @@ struct Plan {
     size_t nseg;
     int shape;
     SegItem* warp_items;
-    SegItem* block_items;
+    SegItem* cls_items;
     SegDesc* big;
     SegCtl* ctl;
-    uint32_t n_big;
-    uint64_t big_keys;
+    SegCtl counts;       // the classification's counts (host copy)
+    uint32_t launches;   // kernels in the graph
     cudaGraph_t graph;
     cudaGraphExec_t exec;
 };
+
+static SegLists plan_lists(const Plan* p) {
+    SegLists L;
+    L.warp_items = p->warp_items;
+    L.cls_items = p->cls_items;
+    L.stride = p->nseg + 1;
+    L.big = p->big;
+    L.ctl = p->ctl;
+    return L;
+}
 
 }  // namespace s512
 
@@ -380,7 +422,7 @@ int s512_segsort_plan_create(s512_segsort_plan** out, int dtype, void* keys, voi
     p->shape = seg_shape_for(dtype);
     // plan-owned lists (the shared scratch pool may be resized by other calls)
     if (cudaMalloc(&p->warp_items, (nseg + 1) * sizeof(SegItem)) != cudaSuccess ||
-        cudaMalloc(&p->block_items, (nseg + 1) * sizeof(SegItem)) != cudaSuccess ||
+        cudaMalloc(&p->cls_items, SEG_NCLASS * (nseg + 1) * sizeof(SegItem)) != cudaSuccess ||
         cudaMalloc(&p->big, (nseg + 1) * sizeof(SegDesc)) != cudaSuccess ||
         cudaMalloc(&p->ctl, sizeof(SegCtl)) != cudaSuccess) {
         cudaGetLastError();
@@ -388,40 +430,35 @@ int s512_segsort_plan_create(s512_segsort_plan** out, int dtype, void* keys, voi
         set_error("s512_segsort_plan_create: allocation failed");
         return S512_ERR_ALLOC;
     }
-    SegLists L{p->warp_items, p->block_items, p->big, p->ctl};
+    const SegLists L = plan_lists(p);
     int rc;
     {
         CallGuard guard(C, st);
         rc = classify(d_offsets, nseg, shape_cap(p->shape), L, st);
-        SegCtl h;
         if (!rc) {
-            S512_CUDA_TRY(cudaMemcpyAsync(&h, p->ctl, sizeof(SegCtl), cudaMemcpyDeviceToHost, st));
+            S512_CUDA_TRY(cudaMemcpyAsync(&p->counts, p->ctl, sizeof(SegCtl), cudaMemcpyDeviceToHost, st));
             S512_CUDA_TRY(cudaStreamSynchronize(st));
-            p->n_big = h.n_big;
-            p->big_keys = h.big_keys;
         }
-        // kernel attributes and grid size are settled before the capture
+        // kernel attributes and grid sizes are settled before the capture
+        uint32_t launches = 0;
         if (!rc) {
-            if (dtype == DT_I32) rc = launch_small_shape(*C, p->shape, make_i32(keys, values), p->warp_items,
-                                                         p->block_items, p->ctl, st, true);
-            else if (dtype == DT_F64) rc = launch_small_shape(*C, p->shape, make_f64(keys, values), p->warp_items,
-                                                              p->block_items, p->ctl, st, true);
-            else rc = launch_small_shape(*C, p->shape, make_kv(keys, values), p->warp_items, p->block_items,
-                                         p->ctl, st, true);
+            if (dtype == DT_I32) rc = launch_classes(*C, p->shape, make_i32(keys, values), L, p->counts, st, &launches,
+                                                     true);
+            else if (dtype == DT_F64) rc = launch_classes(*C, p->shape, make_f64(keys, values), L, p->counts, st,
+                                                          &launches, true);
+            else rc = launch_classes(*C, p->shape, make_kv(keys, values), L, p->counts, st, &launches, true);
         }
-        // capture: reset the queue counters, then the persistent launch
+        // capture the class launches (the lists and counts stay on the device)
         cudaStream_t cs = nullptr;
         if (!rc && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) rc = S512_ERR_CUDA;
         if (!rc) {
             if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = S512_ERR_CUDA;
             if (!rc) {
-                cudaMemsetAsync(&p->ctl->ctr_block, 0, 2 * sizeof(uint32_t), cs);
-                if (dtype == DT_I32) rc = launch_small_shape(*C, p->shape, make_i32(keys, values), p->warp_items,
-                                                             p->block_items, p->ctl, cs);
-                else if (dtype == DT_F64) rc = launch_small_shape(*C, p->shape, make_f64(keys, values),
-                                                                  p->warp_items, p->block_items, p->ctl, cs);
-                else rc = launch_small_shape(*C, p->shape, make_kv(keys, values), p->warp_items, p->block_items,
-                                             p->ctl, cs);
+                if (dtype == DT_I32) rc = launch_classes(*C, p->shape, make_i32(keys, values), L, p->counts, cs,
+                                                         &p->launches);
+                else if (dtype == DT_F64) rc = launch_classes(*C, p->shape, make_f64(keys, values), L, p->counts, cs,
+                                                              &p->launches);
+                else rc = launch_classes(*C, p->shape, make_kv(keys, values), L, p->counts, cs, &p->launches);
                 cudaGraph_t g = nullptr;
                 if (cudaStreamEndCapture(cs, &g) != cudaSuccess) rc = rc ? rc : S512_ERR_CUDA;
                 p->graph = g;
@@ -433,7 +470,7 @@ int s512_segsort_plan_create(s512_segsort_plan** out, int dtype, void* keys, voi
     }
     if (rc) {
         cudaGetLastError();
-        set_error("s512_segsort_plan_create: capture of the persistent launch failed");
+        set_error("s512_segsort_plan_create: capture of the class launches failed");
         s512_segsort_plan_destroy((s512_segsort_plan*)p);
         return rc;
     }
@@ -452,16 +489,16 @@ int s512_segsort_plan_launch(s512_segsort_plan* plan, void* stream) {
     s512_stats& S = thread_stats();
     memset(&S, 0, sizeof(S));
     S512_CUDA_TRY(cudaGraphLaunch(p->exec, st));
-    S.kernel_launches = 1;
-    if (p->n_big) {
+    S.kernel_launches = p->launches;
+    if (p->counts.n_big) {
         PhaseTimer tm(st, false);
-        SegLists L{p->warp_items, p->block_items, p->big, p->ctl};
+        const SegLists L = plan_lists(p);
+        const uint32_t nb = p->counts.n_big;
+        const uint64_t bk = p->counts.big_keys;
         int rc;
-        if (p->dt == DT_I32) rc = sort_big<uint32_t>(*C, make_i32(p->keys, p->values), L, p->n_big, p->big_keys, st,
-                                                     tm, S);
-        else if (p->dt == DT_F64) rc = sort_big<uint64_t>(*C, make_f64(p->keys, p->values), L, p->n_big,
-                                                          p->big_keys, st, tm, S);
-        else rc = sort_big<uint64_t>(*C, make_kv(p->keys, p->values), L, p->n_big, p->big_keys, st, tm, S);
+        if (p->dt == DT_I32) rc = sort_big<uint32_t>(*C, make_i32(p->keys, p->values), L, nb, bk, st, tm, S);
+        else if (p->dt == DT_F64) rc = sort_big<uint64_t>(*C, make_f64(p->keys, p->values), L, nb, bk, st, tm, S);
+        else rc = sort_big<uint64_t>(*C, make_kv(p->keys, p->values), L, nb, bk, st, tm, S);
         if (rc) return rc;
     }
     guard.finish();
@@ -475,7 +512,7 @@ int s512_segsort_plan_destroy(s512_segsort_plan* plan) {
     if (p->exec) cudaGraphExecDestroy(p->exec);
     if (p->graph) cudaGraphDestroy(p->graph);
     cudaFree(p->warp_items);
-    cudaFree(p->block_items);
+    cudaFree(p->cls_items);
     cudaFree(p->big);
     cudaFree(p->ctl);
     delete p;

@@ -2,12 +2,14 @@
 //
 // The reference's analogue is a loop of SmallSort16V (or Sort) over
 // independent arrays (sort512perf.cpp:612-709 timeSmall).  Here a batch of
-// segments is classified once by length, then one persistent launch sorts
-// every segment of up to a block's capacity: blocks first take "block"
-// segments from an atomic queue (one block per segment: the slot sort of
-// s512_slotsort.cuh, with the bitonic + merge-path block sort for segments
-// whose values are unevenly spread), then every warp takes "warp" segments of
-// at most 256 keys (one bitonic network per warp).  Longer segments run the partition levels.
+// segments is classified once by length into size classes: segments of at
+// most 256 keys are sorted one per warp (a bitonic network in registers);
+// longer ones, up to the largest block class, one per block of the smallest
+// class that holds them (the slot sort of s512_slotsort.cuh, with the
+// bitonic + merge-path block sort for segments whose values are unevenly
+// spread), each class by its own persistent launch sized for it, so that a
+// 300-key segment does not pay for the counters of a 16K-key block.  Longer
+// segments run the partition levels.
 #pragma once
 
 #include "s512_blocksort.cuh"
@@ -21,9 +23,13 @@ struct SegItem {
     uint32_t pad_;
 };
 
+// Block classes: class c holds segments of up to 1024 << c keys.
+constexpr int SEG_NCLASS = 5;
+__host__ __device__ constexpr uint32_t seg_class_cap(int c) { return 1024u << c; }
+
 struct SegCtl {
-    uint32_t n_warp, n_block, n_big;
-    uint32_t ctr_block, ctr_warp;
+    uint32_t n_warp, n_big;
+    uint32_t n_cls[SEG_NCLASS];
     uint32_t err;
     unsigned long long big_keys;
 };
@@ -42,9 +48,12 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
     return base + __popc(m & ((1u << lane_id()) - 1u));
 }
 
-__global__ void segsort_classify_kernel(const size_t* __restrict__ offsets, size_t nseg, uint32_t block_cap,
-                                        SegItem* __restrict__ warp_items, SegItem* __restrict__ block_items,
-                                        SegDesc* __restrict__ big, SegCtl* __restrict__ ctl) {
+// Segments of 2..256 keys to the warp list, of up to max_cap keys to the list
+// of the smallest block class that holds them (class c's list starts at
+// cls_items + c * cls_stride), longer ones to the partition list.
+__global__ void segsort_classify_kernel(const size_t* __restrict__ offsets, size_t nseg, uint32_t max_cap,
+                                        SegItem* __restrict__ warp_items, SegItem* __restrict__ cls_items,
+                                        size_t cls_stride, SegDesc* __restrict__ big, SegCtl* __restrict__ ctl) {
     const size_t stride = (size_t)gridDim.x * blockDim.x;
     for (size_t base = (size_t)blockIdx.x * blockDim.x; base < nseg; base += stride) {
         const size_t i = base + threadIdx.x;
@@ -54,13 +63,21 @@ __global__ void segsort_classify_kernel(const size_t* __restrict__ offsets, size
             len = offsets[i + 1] - off;
         }
         const bool w = len > 1 && len <= (uint64_t)WARP_SEG_MAX;
-        const bool b = len > (uint64_t)WARP_SEG_MAX && len <= block_cap;
-        const bool g = len > block_cap;
+        const bool blk = len > (uint64_t)WARP_SEG_MAX && len <= max_cap;
+        const bool g = len > max_cap;
+        int cls = -1;
+        if (blk) {
+            cls = 0;
+            while (seg_class_cap(cls) < len) ++cls;
+        }
         const uint32_t sw = warp_append(&ctl->n_warp, w);
-        const uint32_t sb = warp_append(&ctl->n_block, b);
         const uint32_t sg = warp_append(&ctl->n_big, g);
         if (w) warp_items[sw] = SegItem{off, (uint32_t)len, 0u};
-        if (b) block_items[sb] = SegItem{off, (uint32_t)len, 0u};
+#pragma unroll
+        for (int c = 0; c < SEG_NCLASS; ++c) {
+            const uint32_t sc = warp_append(&ctl->n_cls[c], cls == c);
+            if (cls == c) cls_items[(size_t)c * cls_stride + sc] = SegItem{off, (uint32_t)len, 0u};
+        }
         if (g) {
             SegDesc d;
             d.in_off = off;
@@ -75,47 +92,18 @@ __global__ void segsort_classify_kernel(const size_t* __restrict__ offsets, size
     }
 }
 
-// The persistent launch for warp and block segments.  io reads and writes the
-// caller's layout in place.
-template <typename Codec, int THREADS, int EPT>
-__global__ void __launch_bounds__(THREADS, 1024 / THREADS) segsort_small_kernel(Codec io, const SegItem* __restrict__ warp_items,
-                                                                const SegItem* __restrict__ block_items,
-                                                                SegCtl* __restrict__ ctl) {
+// Warp segments: one warp per segment (8 warps per block), in place on the
+// caller's layout.
+template <typename Codec>
+__global__ void __launch_bounds__(256) segsort_warp_kernel(Codec io, const SegItem* __restrict__ items,
+                                                           const SegCtl* __restrict__ ctl) {
     using K = typename Codec::Key;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    K* s = reinterpret_cast<K*>(smem_raw);
-    __shared__ uint32_t s_item;
-    __shared__ SlotRed<K> red;
-    const uint32_t nblock = ctl->n_block;
-    const uint32_t nwarp = ctl->n_warp;
-
-    // block segments
-    while (true) {
-        if (threadIdx.x == 0) s_item = atomicAdd(&ctl->ctr_block, 1u);
-        __syncthreads();
-        const uint32_t it = s_item;
-        __syncthreads();
-        if (it >= nblock) break;
-        const SegItem item = block_items[it];
-        K key[EPT];
-#pragma unroll
-        for (int r = 0; r < EPT; ++r) {
-            const uint32_t i = (uint32_t)r * THREADS + threadIdx.x;
-            if (i < item.count) key[r] = io.load(item.off + i);
-        }
-        block_slot_sort<K, THREADS, EPT, true>(
-            key, item.count, [&](uint32_t i, K x) { io.store(item.off + i, x); }, [] {}, [] {}, smem_raw, red);
-    }
-
-    // warp segments
+    __shared__ K stage[8][WARP_REGION];
+    const uint32_t nitems = ctl->n_warp;
     const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
-    K* sw = s + (size_t)warp * WARP_REGION;
-    while (true) {
-        uint32_t w = 0;
-        if (lane == 0) w = atomicAdd(&ctl->ctr_warp, 1u);
-        w = __shfl_sync(0xFFFFFFFFu, w, 0);
-        if (w >= nwarp) break;
-        const SegItem item = warp_items[w];
+    K* sw = stage[warp];
+    for (uint32_t w = blockIdx.x * 8 + warp; w < nitems; w += gridDim.x * 8) {
+        const SegItem item = items[w];
         for (uint32_t i = lane; i < (uint32_t)WARP_SEG_MAX; i += 32)
             sw[pidx(i)] = i < item.count ? io.load(item.off + i) : KeyMax<K>::value;
         __syncwarp();
@@ -128,6 +116,41 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) segsort_small_kernel(
         __syncwarp();
         for (uint32_t i = lane; i < item.count; i += 32) io.store(item.off + i, sw[pidx(i)]);
         __syncwarp();
+    }
+}
+
+// One block class: one block per segment of at most THREADS * EPT keys; the
+// next segment's keys are loaded into registers while the current one is
+// ranked and written.
+template <typename Codec, int THREADS, int EPT>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS)
+    segsort_block_kernel(Codec io, const SegItem* __restrict__ items, const uint32_t* __restrict__ n_items) {
+    using K = typename Codec::Key;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ SlotRed<K> red;
+    const uint32_t nitems = *n_items;
+    uint32_t it = blockIdx.x;
+    if (it >= nitems) return;
+    SegItem cur = items[it];
+    K key[EPT];
+    auto load = [&](const SegItem& item) {
+#pragma unroll
+        for (int r = 0; r < EPT; ++r) {
+            const uint32_t i = (uint32_t)r * THREADS + threadIdx.x;
+            if (i < item.count) key[r] = io.load(item.off + i);
+        }
+    };
+    load(cur);
+    for (; it < nitems; it += gridDim.x) {
+        const uint32_t nx = it + gridDim.x;
+        SegItem next;
+        next.count = 0;
+        if (nx < nitems) next = items[nx];
+        const uint64_t off = cur.off;
+        block_slot_sort<K, THREADS, EPT, true>(
+            key, cur.count, [&](uint32_t i, K x) { io.store(off + i, x); }, [&]() { load(next); }, [] {}, smem_raw,
+            red);
+        cur = next;
     }
 }
 

@@ -26,6 +26,7 @@
 #pragma once
 
 #include <cstddef>
+#include <type_traits>
 
 #include "s512_slotsort.cuh"
 
@@ -354,6 +355,54 @@ __device__ __forceinline__ uint32_t find_bucket(const K* __restrict__ tree, K x,
     return range_b[j];
 }
 
+// A split set's slot map held in registers for a run of lookups: keys are
+// clamped to [lo, lo + range] (one compare: x - lo wraps above range when
+// x < lo), cut to 32 bits by a funnel shift and scaled.  Same slots as
+// SlotMap::operator() on the clamped key.
+template <typename K>
+struct SlotRegs {
+    K lo, range;
+    uint32_t sh, mul;
+    bool direct;
+    __device__ __forceinline__ SlotRegs(const SlotMap<K>& f, K hi)
+        : lo(f.lo), range(hi - f.lo), sh(f.sh), mul(f.mul), direct(f.direct != 0) {}
+    __device__ __forceinline__ uint32_t operator()(K x) const {
+        K d = x - lo;
+        if (d > range) d = x < lo ? K(0) : range;
+        uint32_t d32;
+        if constexpr (sizeof(K) == 8)
+            d32 = __funnelshift_rc((uint32_t)d, (uint32_t)(d >> 32), sh);  // sh <= 32
+        else
+            d32 = (uint32_t)d >> sh;
+        return direct ? d32 : __umulhi(d32, mul);
+    }
+};
+
+// Bucket of key x given its slot entry (see SplitSet::slot_tab).
+template <typename K>
+__device__ __forceinline__ uint32_t bucket_from_slot(uint32_t e, K x, bool has_eq, const K* __restrict__ uniq,
+                                                     const uint8_t* __restrict__ range_b,
+                                                     const uint8_t* __restrict__ eq_b,
+                                                     const uint32_t* __restrict__ eq_mask) {
+    uint32_t lo = e & 0xFFu;
+    const uint32_t cnt = e >> 8;
+    if (cnt) {
+        if (cnt == 1) {  // one splitter shares the key's slot
+            lo += uniq[lo] < x ? 1u : 0u;
+        } else {
+            uint32_t hi = lo + cnt;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (uniq[mid] < x) lo = mid + 1; else hi = mid;
+            }
+        }
+    }
+    const uint32_t j = lo;  // number of unique splitters < x
+    if (!has_eq) return j;
+    if (j < 255 && ((eq_mask[j >> 5] >> (j & 31)) & 1u) && uniq[j] == x) return eq_b[j];
+    return range_b[j];
+}
+
 // The same bucket through the splitter lookup table: the key's slot gives the
 // unique splitters below it and the few that share its slot, which are
 // settled by comparisons with uniq[] (none for most keys).
@@ -627,119 +676,132 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
         const uint32_t tma_elems = a.tma ? ((cnt * ESZ) & ~15u) / ESZ : 0u;
         const bool has_eq = sm.has_eq != 0;
         const bool learned = sm.use_learned != 0;
+        const SlotRegs<K> fm(sm.T.P.fmap, sm.T.P.fhi);  // (meaningless for a learned segment: unused)
 
-        // A. keys (striped: element r*THREADS + tid, from the bulk-copied
-        // tile; tail elements past the copied bytes from global memory),
-        // their buckets and their ranks within the tile
-        K key[IPT];
-        uint32_t br[IPT];  // bucket | rank << 8
+        // a whole tile from the bulk copy (no per-key range checks)
+        const bool FULL = cnt == (uint32_t)TILE && tma_elems == (uint32_t)TILE;
+        {
+            // A. keys (striped: element r*THREADS + tid, from the bulk-copied
+            // tile; tail elements past the copied bytes from global memory),
+            // their buckets and their ranks within the tile
+            K key[IPT];
+            uint32_t br[IPT];  // bucket | rank << 8
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t idx = (uint32_t)(r * THREADS + tid);
-            if (idx < cnt) key[r] = idx < tma_elems ? in.decode(sm.buf[b], idx, TILE) : in.load(base + idx);
-        }
-        // all IPT bucket lookups first: they are independent chains of shared
-        // loads, so the scheduler can overlap them
-        uint32_t bks[IPT];
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t idx = (uint32_t)(r * THREADS + tid);
+                if (FULL) key[r] = in.decode(sm.buf[b], idx, TILE);
+                else if (idx < cnt) key[r] = idx < tma_elems ? in.decode(sm.buf[b], idx, TILE) : in.load(base + idx);
+            }
+            // all IPT bucket lookups first: they are independent chains of
+            // shared loads, so the scheduler can overlap them
+            uint32_t bks[IPT];
+            if (learned) {
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t idx = (uint32_t)(r * THREADS + tid);
-            // lanes past the end of the tile carry the out-of-range bucket NB
-            if (idx >= cnt) bks[r] = (uint32_t)NB;
-            else if (learned)
-                // (only the model prefix of the LearnedSet is in shared memory)
-                bks[r] = learned_bucket<K>(*reinterpret_cast<const LearnedSet<K>*>(sm.T.model), key[r]);
-            else
-                bks[r] = find_bucket_tab<K>(sm.T.P.tab, sm.T.P.fmap, sm.T.P.fhi, key[r], has_eq, sm.T.P.uniq,
-                                            sm.T.P.range_b, sm.T.P.eq_b, sm.T.P.eq_mask);
-        }
-#pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t idx = (uint32_t)(r * THREADS + tid);
-            const bool valid = idx < cnt;
-            const uint32_t bk = bks[r];
-            // warp-uniform bucket (sorted / few-distinct input): one atomic for the warp
-            const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, bk, 0);
-            const bool uni = __all_sync(0xFFFFFFFFu, bk == b0);
-            uint32_t rank = 0;
-            if (uni) {
-                if (b0 < (uint32_t)NB) {
-                    uint32_t basev = 0;
-                    if (lane_id() == 0) basev = atomicAdd(&sm.hist[b0], 32u);
-                    rank = __shfl_sync(0xFFFFFFFFu, basev, 0) + lane_id();
+                for (int r = 0; r < IPT; ++r) {
+                    const uint32_t idx = (uint32_t)(r * THREADS + tid);
+                    // (only the model prefix of the LearnedSet is in shared memory)
+                    bks[r] = (FULL || idx < cnt)
+                                 ? learned_bucket<K>(*reinterpret_cast<const LearnedSet<K>*>(sm.T.model), key[r])
+                                 : (uint32_t)NB;  // lanes past the end carry the out-of-range bucket NB
                 }
-            } else if (valid) {
-                rank = atomicAdd(&sm.hist[bk], 1u);
+            } else {
+#pragma unroll
+                for (int r = 0; r < IPT; ++r) bks[r] = sm.T.P.tab[fm(key[r])];  // slot entries first
+#pragma unroll
+                for (int r = 0; r < IPT; ++r) {
+                    const uint32_t idx = (uint32_t)(r * THREADS + tid);
+                    bks[r] = (FULL || idx < cnt) ? bucket_from_slot<K>(bks[r], key[r], has_eq, sm.T.P.uniq,
+                                                                       sm.T.P.range_b, sm.T.P.eq_b, sm.T.P.eq_mask)
+                                                 : (uint32_t)NB;
+                }
             }
-            br[r] = bk | (rank << 8);
-        }
-        __syncthreads();  // (1) the tile's histogram is complete; the previous tile is written
+#pragma unroll
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t bk = bks[r];
+                // warp-uniform bucket (sorted / few-distinct input): one atomic for the warp
+                const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, bk, 0);
+                const bool uni = __all_sync(0xFFFFFFFFu, bk == b0);
+                uint32_t rank = 0;
+                if (uni) {
+                    if (FULL || b0 < (uint32_t)NB) {
+                        uint32_t basev = 0;
+                        if (lane_id() == 0) basev = atomicAdd(&sm.hist[b0], 32u);
+                        rank = __shfl_sync(0xFFFFFFFFu, basev, 0) + lane_id();
+                    }
+                } else if (FULL || bk < (uint32_t)NB) {
+                    rank = atomicAdd(&sm.hist[bk], 1u);
+                }
+                br[r] = bk | (rank << 8);
+            }
+            __syncthreads();  // (1) the tile's histogram is complete; the previous tile is written
 
-        // B. reserve the tile's share of each bucket's region, and the
-        // buckets' starts within the tile (exclusive scan by warp 0)
-        uint32_t h = 0;
-        unsigned long long off = 0;
-        if (tid < NB) {
-            h = sm.hist[tid];
-            if (h) off = atomicAdd(&a.fill[(size_t)seg * NB + tid], (unsigned long long)h);
-        }
-        if (tid < 32) {
-            uint32_t v[NB / 32];
-            uint32_t run = 0;
-#pragma unroll
-            for (int i = 0; i < NB / 32; ++i) {
-                v[i] = run;
-                run += sm.hist[tid * (NB / 32) + i];
+            // B. reserve the tile's share of each bucket's region, and the
+            // buckets' starts within the tile (exclusive scan by warp 0)
+            uint32_t h = 0;
+            unsigned long long off = 0;
+            if (tid < NB) {
+                h = sm.hist[tid];
+                if (h) off = atomicAdd(&a.fill[(size_t)seg * NB + tid], (unsigned long long)h);
             }
-            uint32_t inc = run;
+            if (tid < 32) {
+                uint32_t v[NB / 32];
+                uint32_t run = 0;
 #pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-                if (tid >= d) inc += o;
+                for (int i = 0; i < NB / 32; ++i) {
+                    v[i] = run;
+                    run += sm.hist[tid * (NB / 32) + i];
+                }
+                uint32_t inc = run;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+                    if (tid >= d) inc += o;
+                }
+                const uint32_t ex = inc - run;
+#pragma unroll
+                for (int i = 0; i < NB / 32; ++i) sm.loc[tid * (NB / 32) + i] = ex + v[i];
             }
-            const uint32_t ex = inc - run;
-#pragma unroll
-            for (int i = 0; i < NB / 32; ++i) sm.loc[tid * (NB / 32) + i] = ex + v[i];
-        }
-        if (tid == 0) {
-            // the next tile's keys into the other buffer: its last reader, the
-            // previous tile's write-out, finished before barrier (1)
-            if (a.tma && t_next < ntiles) issue(t_next, b ^ 1);
-            sm.tile_cur = t_next;
-            t_next = claim();
-        }
-        __syncthreads();  // (2) bucket starts within the tile
+            if (tid == 0) {
+                // the next tile's keys into the other buffer: its last reader,
+                // the previous tile's write-out, finished before barrier (1)
+                if (a.tma && t_next < ntiles) issue(t_next, b ^ 1);
+                sm.tile_cur = t_next;
+                t_next = claim();
+            }
+            __syncthreads();  // (2) bucket starts within the tile
 
-        // C. stage the keys in bucket order, reusing this tile's buffer
-        K* stage = reinterpret_cast<K*>(sm.buf[b]);
+            // C. stage the keys in bucket order, reusing this tile's buffer
+            K* stage = reinterpret_cast<K*>(sm.buf[b]);
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t idx = (uint32_t)(r * THREADS + tid);
-            if (idx < cnt) {
-                const uint32_t bk = br[r] & 0xFFu;
-                const uint32_t p = sm.loc[bk] + (br[r] >> 8);
-                stage[p] = key[r];
-                sm.bkt[p] = (uint8_t)bk;
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t idx = (uint32_t)(r * THREADS + tid);
+                if (FULL || idx < cnt) {
+                    const uint32_t bk = br[r] & 0xFFu;
+                    const uint32_t p = sm.loc[bk] + (br[r] >> 8);
+                    stage[p] = key[r];
+                    sm.bkt[p] = (uint8_t)bk;
+                }
             }
-        }
-        if (tid < NB) {
-            const unsigned long long end = off + h;
-            const bool ovf = !data_ok || end > sm.region_cap[tid];
-            if (ovf && h) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
-            sm.gdelta[tid] = ovf ? GDELTA_DROP : sm.sd.out_base + sm.region_off[tid] + off - (uint64_t)sm.loc[tid];
-            sm.hist[tid] = 0;  // (next used after barrier (3))
-        }
-        if (tid == 0 && !data_ok) sm.abort = 1;
-        __syncthreads();  // (3) staging complete
+            if (tid < NB) {
+                const unsigned long long end = off + h;
+                const bool ovf = !data_ok || end > sm.region_cap[tid];
+                if (ovf && h) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
+                sm.gdelta[tid] =
+                    ovf ? GDELTA_DROP : sm.sd.out_base + sm.region_off[tid] + off - (uint64_t)sm.loc[tid];
+                sm.hist[tid] = 0;  // (next used after barrier (3))
+            }
+            if (tid == 0 && !data_ok) sm.abort = 1;
+            __syncthreads();  // (3) staging complete
 
-        // D. coalesced write-out (an overflowed bucket's keys are dropped: the
-        // level is redone)
+            // D. coalesced write-out (an overflowed bucket's keys are dropped:
+            // the level is redone)
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            const uint32_t i = (uint32_t)(r * THREADS + tid);
-            if (i < cnt) {
-                const uint64_t g = sm.gdelta[sm.bkt[i]];
-                if (g != GDELTA_DROP) a.out[g + i] = stage[i];
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t i = (uint32_t)(r * THREADS + tid);
+                if (FULL || i < cnt) {
+                    const uint64_t g = sm.gdelta[sm.bkt[i]];
+                    if (g != GDELTA_DROP) a.out[g + i] = stage[i];
+                }
             }
         }
         b ^= 1;

@@ -184,8 +184,10 @@ S512_API int s512_sort_omp_merge_f64(double* data, size_t n, int nparts, int fla
  *     nseg segments, offsets has nseg+1 entries (host or device memory; host
  *     data needs host offsets).  Every segment is sorted in place.  The
  *     reference's analogue is a loop of SmallSort16V / Sort over independent
- *     arrays (sort512perf.cpp:612-709, timeSmall).  One persistent launch sorts
- *     all segments that fit a block; longer ones run the partition levels. */
+ *     arrays (sort512perf.cpp:612-709, timeSmall).  Segments of up to 256
+ *     keys are sorted one per warp, longer ones one per block of the smallest
+ *     size class that holds them (1K, 2K, 4K, 8K, 16K keys), one persistent
+ *     launch per class; longer ones run the partition levels. */
 S512_API int s512_segsort_i32(int* data, const size_t* offsets, size_t nseg, int flags, void* stream);
 S512_API int s512_segsort_f64(double* data, const size_t* offsets, size_t nseg, int flags, void* stream);
 S512_API int s512_segsort_kv_i32(int* keys, int* values, const size_t* offsets, size_t nseg, int flags,
@@ -194,9 +196,10 @@ S512_API int s512_segsort_kv_i32(int* keys, int* values, const size_t* offsets, 
 /* Element types of the plan / tuning calls. */
 enum { S512_DTYPE_I32 = 0, S512_DTYPE_F64 = 1, S512_DTYPE_KV_I32 = 2 };
 
-/* Pick the persistent launch's block shape (threads x keys per thread) for a
- * dtype by timing every candidate on random keys with this segment layout
- * (device offsets).  The choice is kept for the process and, when the
+/* Pick the largest block class used (shape 0..3: 2K, 4K, 8K or 16K keys;
+ * longer segments run the partition levels) for a dtype by timing every
+ * candidate on random keys with this segment layout (device offsets).  The
+ * choice is kept for the process and, when the
  * environment variable S512_TUNE_CACHE names a file, appended to it and read
  * back by later processes. */
 S512_API int s512_segsort_tune(int dtype, const size_t* d_offsets, size_t nseg, double* best_ms, int* shape_index,
@@ -204,9 +207,10 @@ S512_API int s512_segsort_tune(int dtype, const size_t* d_offsets, size_t nseg, 
 
 /* A segmented sort captured in a CUDA graph for repeated use on the same
  * device buffers and layout: classification happens once at creation; each
- * launch replays the persistent kernel (and runs the partition levels for
- * segments longer than a block, which are not captured).  values is used by
- * S512_DTYPE_KV_I32 only. */
+ * launch replays the captured class launches (and runs the partition levels
+ * for segments longer than the largest class, which are not captured: their
+ * level structure depends on the data).  values is used by S512_DTYPE_KV_I32
+ * only. */
 typedef struct s512_segsort_plan s512_segsort_plan;
 S512_API int s512_segsort_plan_create(s512_segsort_plan** plan, int dtype, void* keys, void* values,
                                       const size_t* d_offsets, size_t nseg, void* stream);

@@ -28,8 +28,9 @@ def test_segsort_host_matches_restatement(dt, s512, cuda, oracle):
 
 def test_segsort_edge_layouts(s512, cuda, oracle):
     import workloads
-    # empty segments, single keys, exactly 256 / 257, a block limit, a long one
-    lens = [0, 1, 2, 0, 255, 256, 257, 4096, 8192, 8193, 16385, 70000, 3, 0]
+    # empty segments, single keys, exactly 256 / 257, every block class's
+    # limit and one past it, long ones
+    lens = [0, 1, 2, 0, 255, 256, 257, 1024, 1025, 2048, 2049, 4096, 4097, 8192, 8193, 16384, 16385, 70000, 3, 0]
     off = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
     a = workloads.uniform_i32_np(int(off[-1]), 7)
     a[1000:1500] = 42  # a run of equal keys
