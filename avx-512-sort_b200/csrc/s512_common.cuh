@@ -282,21 +282,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
         : "memory");
     return ok != 0;
 }
-// 1-D bulk store shared -> global (TMA, no multicast), tracked per thread in
-// bulk async-groups.  dst and src 16-byte aligned, bytes a multiple of 16;
-// shared memory written by the generic proxy must be fenced
-// (fence_proxy_async_smem) by its writers before the copy reads it.
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_u32(src)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// this thread's bulk stores have finished reading shared memory
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-// this thread's bulk stores are complete
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-
 // bounded wait for a phase of an mbarrier; false if the limit was reached
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
     for (uint32_t i = 0; i < SPIN_LIMIT; ++i)

@@ -78,7 +78,9 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
     S512_CUDA_TRY(cudaMemcpyAsync(seg, &sd, sizeof(sd), cudaMemcpyHostToDevice, st));
     splitter_kernel<K><<<1, NB, 0, st>>>(samples, seg, 1, ss, KB);
     S512_LAUNCH_CHECK();
-    learned_fit_kernel<K><<<1, LR_THREADS, 0, st>>>(samples, seg, 1, ss, ls, KB, (float)config().max_imbalance);
+    uint32_t* lfirst = (uint32_t*)C->get("lr_fit_first", (LR_LEAVES + 1) * sizeof(uint32_t));
+    if (!lfirst) return S512_ERR_ALLOC;
+    launch_learned_fit<K>(samples, seg, 1, ss, ls, lfirst, KB, (float)config().max_imbalance, st, 1);
     S512_LAUNCH_CHECK();
     if (d_hist) {
         S512_CUDA_TRY(cudaMemsetAsync(d_hist, 0, NB * sizeof(uint32_t), st));
@@ -87,7 +89,7 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
     }
     struct {
         float loss_init, loss_root, loss_final, max_over_mean;
-        uint32_t nbuckets, nmodel, ok;
+        uint32_t nbuckets, nmodel, ok, balanced;
     } h;
     const LearnedSet<K>* lp = ls;
     S512_CUDA_TRY(cudaMemcpyAsync(&h.loss_init, &lp->loss_init, 3 * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -95,6 +97,7 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
     S512_CUDA_TRY(cudaMemcpyAsync(&h.nbuckets, &lp->nbuckets, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaMemcpyAsync(&h.nmodel, &lp->nmodel, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaMemcpyAsync(&h.ok, &lp->ok, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    S512_CUDA_TRY(cudaMemcpyAsync(&h.balanced, &lp->balanced, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     S512_CUDA_TRY(cudaStreamSynchronize(st));
     guard.finish();
     out->loss_init = h.loss_init;
@@ -104,7 +107,7 @@ static int fit(const void* d_keys, uint32_t m, uint64_t seg_count, uint32_t* d_h
     out->nbuckets = h.nbuckets;
     out->nmodel = h.nmodel;
     out->ok = h.ok;
-    out->pad_ = 0;
+    out->balanced = h.balanced;
     return S512_OK;
 }
 

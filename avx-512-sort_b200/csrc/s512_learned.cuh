@@ -19,14 +19,24 @@
 // splitters' equality buckets) splits its model bucket into below / equal /
 // above, and its equal bucket needs no sort.
 //
-// Training (learned_fit_kernel, one block per segment): targets are the
+// Training (on the device, per segment): targets are the
 // sample's empirical CDF y_i = (i + 0.5) / m.  The root starts from the
 // sample histogram over its R pieces and takes ITERS full-batch Adam steps on
 // theta with the analytic gradient
 //   dL/dw_t = (2/m) * ( sum_{i: s_i > t} r_i + sum_{i: s_i = t} r_i * frac_i ),
 //   dL/dtheta_t = dL/dw_t * 2 * theta_t,         r_i = p0(z_i) - y_i.
-// Each leaf starts from its least-squares line on the samples routed to it and
-// takes LEAF_ITERS Adam steps on (a, beta) with b = beta^2.
+// Each leaf starts from its least-squares line on the samples routed to it,
+// which is already the optimum of its squared error when its slope is
+// positive; a leaf whose least-squares slope was clipped to 0 takes
+// LEAF_ITERS Adam steps on (a, beta) with b = beta^2.
+//
+// The fit is three launches: the roots (one block per segment), the leaves
+// (one warp per (segment, leaf), all segments at once), and the bucket layout
+// (one block per segment).  A segment is routed by its model only when the
+// model passes the balance check AND the plain splitter table would have to
+// search for many keys (more than LR_TABLE_SEARCH_FRAC of the sample falls in
+// slots shared by several splitters, as with tightly clustered keys): where
+// the table settles a key with one lookup the model has nothing to win.
 #pragma once
 
 #include "s512_blocksort.cuh"
@@ -44,6 +54,7 @@ constexpr int LR_THREADS = 512;
 constexpr int LR_ITERS = 16;
 constexpr int LR_LEAF_ITERS = 8;
 constexpr float LR_STEP = 0.02f;  // Adam step, relative to the parameters' scale
+constexpr float LR_TABLE_SEARCH_FRAC = 0.25f;
 
 template <typename K>
 struct LeafParam {
@@ -69,8 +80,10 @@ struct LearnedSet {
     uint64_t region_cap[NB];
     uint32_t bucket_eq[NB / 32];
     uint32_t nbuckets;
-    uint32_t ok;         // 1: accepted (imbalance within bound)
-    uint32_t pad_;
+    uint32_t ok;         // 1: the model routes the segment (balanced, and cheaper than the splitter table)
+    uint32_t balanced;   // 1: imbalance within the bound
+    uint32_t fitted;     // 1: trained (0: too small, or the splitter table needs no searches)
+    uint32_t searches;   // 1: the splitter table would search for many of the segment's keys
     float loss_init, loss_root, loss_final;
     float max_over_mean;  // sample-count imbalance of the learned buckets
 };
@@ -198,36 +211,56 @@ __device__ void root_forward_backward(const K* smp, uint32_t m, K kmin, float in
     __syncthreads();
 }
 
-// One block (LR_THREADS) per segment.  The plain split set of the segment
-// (already computed from the same sorted sample) supplies the heavy keys.
+// --- fit, launch 1: the root of each segment (one block of LR_THREADS each).
+// Also the first sample of each leaf (samples are sorted and routing is
+// monotone, so each leaf owns a contiguous run of the sample), into
+// lfirst[seg * (LR_LEAVES + 1) + l].
 template <typename K>
-__global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __restrict__ samples,
-                                                                 const SegDesc* __restrict__ segs, uint32_t nsegs,
-                                                                 const SplitSet<K>* __restrict__ plain,
-                                                                 LearnedSet<K>* __restrict__ out, int key_bytes,
-                                                                 float max_imbalance) {
+__global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __restrict__ samples,
+                                                                  const SegDesc* __restrict__ segs, uint32_t nsegs,
+                                                                  const SplitSet<K>* __restrict__ plain,
+                                                                  LearnedSet<K>* __restrict__ out,
+                                                                  uint32_t* __restrict__ lfirst, int key_bytes,
+                                                                  int force) {
     const uint32_t sgi = blockIdx.x;
     if (sgi >= nsegs) return;
     __shared__ float theta[LR_ROOT], rw[LR_ROOT], rc[LR_ROOT], gw[LR_ROOT], S0[LR_ROOT], S1[LR_ROOT];
-    __shared__ float loss_acc;
-    __shared__ uint32_t leaf_first[LR_LEAVES + 1];
-    __shared__ uint32_t hist[NB];
-    __shared__ uint32_t wt32[32];
-    __shared__ uint64_t wt64[32];
-    __shared__ uint32_t nheavy_s, max_s, nonempty_s;
-    __shared__ LearnedSet<K> L;  // built here, copied out at the end
-
+    __shared__ float loss_acc, loss_init_s;
+    __shared__ uint32_t search_s;
     const SegDesc sd = segs[sgi];
     const int tid = threadIdx.x;
-    if (sd.count < LR_MIN_KEYS) {  // too small to repay a fit: the split set routes it
-        if (tid == 0) out[sgi].ok = 0;
-        return;
-    }
+    LearnedSet<K>& L = out[sgi];
     const int nb = target_buckets(key_bytes, sd.count);
     const uint32_t m = sample_size(nb);
     const K* smp = samples + (size_t)sgi * SAMPLE_N;
-
-    // coordinate
+    // worth a fit?  Only for a large segment whose splitter table would have
+    // to search for many keys (slots shared by several splitters)
+    if (tid == 0) search_s = 0;
+    __syncthreads();
+    bool fit = sd.count >= LR_MIN_KEYS;
+    bool searches = false;
+    if (fit) {
+        const SplitSet<K>& ps = plain[sgi];
+        const SlotMap<K> fmap = ps.slot_map;
+        uint32_t mine = 0;
+        for (uint32_t i = tid; i < m; i += blockDim.x) {
+            const K xc = kmin(kmax(smp[i], fmap.lo), ps.slot_hi);
+            mine += (ps.slot_tab[fmap(xc)] >> 8) > 1u ? 1u : 0u;
+        }
+        atomicAdd(&search_s, mine);
+        __syncthreads();
+        searches = (float)search_s > LR_TABLE_SEARCH_FRAC * (float)m;
+        fit = searches || force;
+    }
+    if (!fit) {  // the split set routes it
+        if (tid == 0) {
+            L.ok = 0;
+            L.balanced = 0;
+            L.fitted = 0;
+            L.searches = searches ? 1u : 0u;
+        }
+        return;
+    }
     const K kmin = smp[0], kmax = smp[m - 1];
     const K range = kmax - kmin;
     const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
@@ -261,23 +294,30 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
 
     // Adam on theta; the parameters with the lowest loss seen are kept, so
     // training never ends worse than the histogram start
+    static_assert(LR_ROOT == 64, "two root pieces per lane of warp 0");
     Adam opt;
     float best_theta = tid < LR_ROOT ? theta[tid] : 0.f;
     float best_loss = 3.4e38f;
     for (int it = 0; it <= LR_ITERS; ++it) {
-        if (tid < LR_ROOT) rw[tid] = theta[tid] * theta[tid];
-        __syncthreads();
-        if (tid == 0) {
-            float c = 0.f;
-            for (int t = 0; t < LR_ROOT; ++t) {
-                rc[t] = c;
-                c += rw[t];
+        // slopes and their running sums (rc) by warp 0, two pieces a lane
+        if (tid < 32) {
+            const float w0 = theta[2 * tid] * theta[2 * tid], w1 = theta[2 * tid + 1] * theta[2 * tid + 1];
+            float inc = w0 + w1;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const float o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+                if (tid >= d) inc += o;
             }
+            const float ex = inc - (w0 + w1);
+            rw[2 * tid] = w0;
+            rw[2 * tid + 1] = w1;
+            rc[2 * tid] = ex;
+            rc[2 * tid + 1] = ex + w0;
         }
         __syncthreads();
         root_forward_backward<K>(smp, m, kmin, inv_range, rc, rw, S0, S1, &loss_acc, gw);
         const float loss = loss_acc;
-        if (it == 0 && tid == 0) L.loss_init = loss;
+        if (it == 0 && tid == 0) loss_init_s = loss;
         if (loss < best_loss) {
             best_loss = loss;
             if (tid < LR_ROOT) best_theta = theta[tid];
@@ -287,13 +327,9 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
         __syncthreads();
     }
     __syncthreads();
-    if (tid < LR_ROOT) {
-        theta[tid] = best_theta;
-        rw[tid] = best_theta * best_theta;
-    }
-    if (tid == 0) L.loss_root = best_loss;
+    // the kept root, normalised so that it spans [0, 1]
+    if (tid < LR_ROOT) rw[tid] = best_theta * best_theta;
     __syncthreads();
-    // normalise the root so that it spans [0, 1]
     if (tid == 0) {
         float tot = 0.f;
         for (int t = 0; t < LR_ROOT; ++t) tot += rw[t];
@@ -306,212 +342,275 @@ __global__ void __launch_bounds__(LR_THREADS) learned_fit_kernel(const K* __rest
         }
         L.kmin = kmin;
         L.inv_range = inv_range;
+        L.loss_init = loss_init_s;
+        L.loss_root = best_loss;
+        L.fitted = 1;
+        L.searches = searches ? 1u : 0u;
     }
     __syncthreads();
-
-    // leaves: samples are sorted and routing is monotone, so each leaf owns a
-    // contiguous run of the sample; find the run starts
-    for (int l = tid; l <= LR_LEAVES; l += blockDim.x) leaf_first[l] = m;
+    uint32_t* lf = lfirst + (size_t)sgi * (LR_LEAVES + 1);
+    for (int l = tid; l <= LR_LEAVES; l += blockDim.x) lf[l] = m;
     __syncthreads();
     for (uint32_t i = tid; i < m; i += blockDim.x) {
         const int l = leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i]));
         const int lp = i == 0 ? -1 : leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i - 1]));
-        for (int q = lp + 1; q <= l; ++q) leaf_first[q] = i;  // leaves lp+1..l start at i
+        for (int q = lp + 1; q <= l; ++q) lf[q] = i;  // leaves lp+1..l start at i
     }
-    __syncthreads();
-    // one warp per leaf at a time: the lanes stride over the leaf's
-    // (contiguous) samples and every sum is reduced across the warp and taken
-    // from lane 0, so all lanes step the same parameters.  (A leaf can own
-    // most of the sample when the root is skewed; one thread per leaf would
-    // then walk it alone, once per step.)
-    {
-        const int lane = tid & 31, wid = tid >> 5, nw = (int)(blockDim.x >> 5);
-        auto wsum = [&](float v) {
+}
+
+// --- fit, launch 2: the leaves, one warp per (segment, leaf), 8 warps a
+// block.  The lanes stride over the leaf's (contiguous) samples and every sum
+// is reduced across the warp, so all lanes hold the same parameters.
+template <typename K>
+__global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__ samples,
+                                                           const SegDesc* __restrict__ segs, uint32_t nsegs,
+                                                           LearnedSet<K>* __restrict__ out,
+                                                           const uint32_t* __restrict__ lfirst, int key_bytes) {
+    const uint32_t wg = blockIdx.x * 8 + (threadIdx.x >> 5);
+    const uint32_t sgi = wg / LR_LEAVES;
+    const int l = (int)(wg % LR_LEAVES);
+    if (sgi >= nsegs) return;
+    if (!out[sgi].fitted) return;
+    const SegDesc sd = segs[sgi];
+    const int lane = threadIdx.x & 31;
+    const uint32_t m = sample_size(target_buckets(key_bytes, sd.count));
+    const K* smp = samples + (size_t)sgi * SAMPLE_N;
+    auto wsum = [&](float v) {
 #pragma unroll
-            for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
-            return __shfl_sync(0xFFFFFFFFu, v, 0);
-        };
-        for (int l = wid; l < LR_LEAVES; l += nw) {
-            const uint32_t f = leaf_first[l];
-            // leaf_first[q] = first sample routed to a leaf >= q, so leaf l owns
-            // the samples [leaf_first[l], leaf_first[l+1])
-            const uint32_t e = leaf_first[l + 1];
-            LeafParam<K> P;
-            if (f < e && f < m) {
-                const K base = smp[f];
-                const K span = smp[e - 1] - base;
-                const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
-                // least squares on (u, y), u in [0, 1]
-                float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
-                const float cnt = (float)(e - f);
+        for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
+        return v;
+    };
+    // leaf l owns the samples [lfirst[l], lfirst[l+1])
+    const uint32_t* lf = lfirst + (size_t)sgi * (LR_LEAVES + 1);
+    const uint32_t f = lf[l];
+    const uint32_t e = lf[l + 1];
+    LeafParam<K> P;
+    if (f < e && f < m) {
+        const K base = smp[f];
+        const K span = smp[e - 1] - base;
+        const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
+        // least squares on (u, y), u in [0, 1]
+        float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
+        const float cnt = (float)(e - f);
+        for (uint32_t i = f + lane; i < e; i += 32) {
+            const float u = key_to_float(smp[i] - base) * inv_span;
+            const float y = ((float)i + 0.5f) / (float)m;
+            su += u;
+            sy += y;
+            suu += u * u;
+            suy += u * y;
+        }
+        su = wsum(su);
+        sy = wsum(sy);
+        suu = wsum(suu);
+        suy = wsum(suy);
+        const float mu = su / cnt, my = sy / cnt;
+        const float var = suu / cnt - mu * mu, cov = suy / cnt - mu * my;
+        float b = var > 1e-12f ? cov / var : 0.f;
+        const bool clipped = !(b > 0.f);
+        b = clipped ? 0.f : b;
+        float a = my - b * mu;
+        float beta = sqrtf(b);
+        if (clipped) {
+            // refine (a, beta), b = beta^2, by Adam on the leaf's squared
+            // error (forward + backward per step); keep the best pair seen
+            float best_a = a, best_beta = beta, best_l = 3.4e38f;
+            Adam oa, ob;
+            for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
+                float ga = 0.f, gb = 0.f, l2 = 0.f;
                 for (uint32_t i = f + lane; i < e; i += 32) {
                     const float u = key_to_float(smp[i] - base) * inv_span;
-                    const float y = ((float)i + 0.5f) / (float)m;
-                    su += u;
-                    sy += y;
-                    suu += u * u;
-                    suy += u * y;
+                    const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
+                    l2 += r * r;
+                    ga += r;
+                    gb += r * u;
                 }
-                su = wsum(su);
-                sy = wsum(sy);
-                suu = wsum(suu);
-                suy = wsum(suy);
-                const float mu = su / cnt, my = sy / cnt;
-                const float var = suu / cnt - mu * mu, cov = suy / cnt - mu * my;
-                float b = var > 1e-12f ? cov / var : 0.f;
-                b = b > 0.f ? b : 0.f;
-                float a = my - b * mu;
-                // refine (a, beta), b = beta^2, by Adam on the leaf's squared
-                // error (forward + backward per step); keep the best pair seen
-                float beta = sqrtf(b);
-                float best_a = a, best_beta = beta, best_l = 3.4e38f;
-                Adam oa, ob;
-                for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
-                    float ga = 0.f, gb = 0.f, l2 = 0.f;
-                    for (uint32_t i = f + lane; i < e; i += 32) {
-                        const float u = key_to_float(smp[i] - base) * inv_span;
-                        const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
-                        l2 += r * r;
-                        ga += r;
-                        gb += r * u;
-                    }
-                    l2 = wsum(l2);
-                    ga = wsum(ga);
-                    gb = wsum(gb);
-                    if (l2 < best_l) {
-                        best_l = l2;
-                        best_a = a;
-                        best_beta = beta;
-                    }
-                    if (it > LR_LEAF_ITERS) break;
-                    ga *= 2.f / cnt;
-                    gb *= 2.f / cnt * 2.f * beta;
-                    a -= oa.step(ga, LR_STEP / (float)m, it);
-                    beta -= ob.step(gb, LR_STEP / (float)m, it);
+                l2 = wsum(l2);
+                ga = wsum(ga);
+                gb = wsum(gb);
+                if (l2 < best_l) {
+                    best_l = l2;
+                    best_a = a;
+                    best_beta = beta;
                 }
-                a = best_a;
-                beta = best_beta;
-                P.base = base;
-                P.a = a;
-                P.b = beta * beta * inv_span;  // slope per unit of (key - base)
-                P.lo = ((float)f + 0.5f) / (float)m;
-                P.hi = ((float)(e - 1) + 0.5f) / (float)m;
-            } else {
-                P.base = KeyMax<K>::value;
-                P.a = 0.f;
-                P.b = 0.f;
-                P.lo = P.hi = -1.f;  // patched below: an empty leaf repeats its left neighbour's top
+                if (it > LR_LEAF_ITERS) break;
+                ga *= 2.f / cnt;
+                gb *= 2.f / cnt * 2.f * beta;
+                a -= oa.step(ga, LR_STEP / (float)m, it);
+                beta -= ob.step(gb, LR_STEP / (float)m, it);
             }
-            if (lane == 0) L.leaf[l] = P;
+            a = best_a;
+            beta = best_beta;
         }
+        P.base = base;
+        P.a = a;
+        P.b = beta * beta * inv_span;  // slope per unit of (key - base)
+        P.lo = ((float)f + 0.5f) / (float)m;
+        P.hi = ((float)(e - 1) + 0.5f) / (float)m;
+    } else {
+        P.base = KeyMax<K>::value;
+        P.a = 0.f;
+        P.b = 0.f;
+        P.lo = P.hi = -1.f;  // patched in launch 3: an empty leaf repeats its left neighbour's top
     }
-    __syncthreads();
-    if (tid == 0) {
-        float last = 0.f;
-        for (int l = 0; l < LR_LEAVES; ++l) {
-            if (L.leaf[l].lo < 0.f) {
-                L.leaf[l].lo = L.leaf[l].hi = last;
-                L.leaf[l].a = last;
-            } else {
-                last = L.leaf[l].hi;
-            }
-        }
-    }
-    __syncthreads();
+    if (lane == 0) out[sgi].leaf[l] = P;
+}
 
-    // buckets: heavy keys from the plain split set (splitters with an equality bucket)
-    const SplitSet<K>& ps = plain[sgi];
-    if (tid == 0) nheavy_s = 0;
-    __syncthreads();
-    uint32_t heavy_mine = 0;
-    if (tid < NB && tid < (int)ps.nuniq) heavy_mine = (ps.eq_mask[tid >> 5] >> (tid & 31)) & 1u;
-    const uint32_t nheavy = __syncthreads_count(heavy_mine != 0);
-    uint32_t nmodel = NB - 2 * nheavy;
-    if (nmodel > (uint32_t)(2 * nb)) nmodel = 2 * nb;  // no more model buckets than the plain path aims for
-    if (nmodel < 2) nmodel = 2;
-    if (tid < NB) {
-        L.heavy_flag[tid] = 0;
-        L.heavy[tid] = K(0);
+// --- fit, launch 3: per segment (one block of NB threads) the empty leaves
+// patched, the heavy keys and bucket ids, the sample's bucket histogram, the
+// balance check, the routing choice, the regions and the final loss.  The
+// plain split set of the segment (computed from the same sorted sample)
+// supplies the heavy keys and the table the routing choice compares with.
+template <typename K>
+__global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict__ samples,
+                                                            const SegDesc* __restrict__ segs, uint32_t nsegs,
+                                                            const SplitSet<K>* __restrict__ plain,
+                                                            LearnedSet<K>* __restrict__ out, int key_bytes,
+                                                            float max_imbalance) {
+    const uint32_t sgi = blockIdx.x;
+    if (sgi >= nsegs) return;
+    if (!out[sgi].fitted) return;
+    const SegDesc sd = segs[sgi];
+    __shared__ LearnedSet<K> L;  // built here, copied out at the end
+    __shared__ uint32_t hist[NB];
+    __shared__ uint32_t first_heavy[NB];
+    __shared__ uint32_t wt32[32];
+    __shared__ uint64_t wt64[32];
+    __shared__ uint32_t max_s, nonempty_s;
+    __shared__ float loss_s, top_w[NB / 32];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(out + sgi);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&L);
+        for (uint32_t i = tid; i < sizeof(LearnedSet<K>) / 4; i += blockDim.x) dst[i] = src[i];
     }
-    __syncthreads();
-    if (tid == 0) {
-        L.nmodel = nmodel;
-        // heavy keys in ascending order; a model bucket keeps its first heavy key
-        for (uint32_t j = 0; j < ps.nuniq && j < (uint32_t)NB; ++j) {
-            if (!((ps.eq_mask[j >> 5] >> (j & 31)) & 1u)) continue;
-            const K h = ps.uniq[j];
-            const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, h);
-            const uint32_t r = model_bucket<K>(leaf_p<K>(L.leaf[leaf_of<K>(p0)], h), nmodel);
-            if (!L.heavy_flag[r]) {
-                L.heavy_flag[r] = 1;
-                L.heavy[r] = h;
-            }
-        }
-        uint32_t id = 0;
-        for (uint32_t r = 0; r < NB; ++r) {
-            L.base_id[r] = (uint8_t)(id < NB ? id : NB - 1);
-            if (r < nmodel) id += L.heavy_flag[r] ? 3u : 1u;
-        }
-        L.nbuckets = id;
-    }
-    __syncthreads();
-
-    // sample counts per learned bucket -> imbalance, capacities, regions
-    if (tid < NB) hist[tid] = 0;
+    const int nb = target_buckets(key_bytes, sd.count);
+    const uint32_t m = sample_size(nb);
+    const K* smp = samples + (size_t)sgi * SAMPLE_N;
     if (tid == 0) {
         max_s = 0;
         nonempty_s = 0;
+        loss_s = 0.f;
     }
     __syncthreads();
+
+    // empty leaves: lo = hi = a = the top of the nearest non-empty leaf to
+    // their left (0 if none): a running maximum of the leaves' tops
+    static_assert(LR_LEAVES == NB, "one thread per leaf");
+    {
+        const bool empty = L.leaf[tid].lo < 0.f;
+        float run = empty ? 0.f : L.leaf[tid].hi;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const float o = __shfl_up_sync(0xFFFFFFFFu, run, d);
+            if (lane >= d) run = fmaxf(run, o);
+        }
+        if (lane == 31) top_w[warp] = run;
+        __syncthreads();
+        for (int w = 0; w < warp; ++w) run = fmaxf(run, top_w[w]);
+        __syncthreads();
+        if (empty) {
+            L.leaf[tid].lo = L.leaf[tid].hi = run;
+            L.leaf[tid].a = run;
+        }
+    }
+    __syncthreads();
+
+    // heavy keys (splitters with an equality bucket in the plain split set):
+    // a model bucket keeps its first heavy key
+    const SplitSet<K>& ps = plain[sgi];
+    first_heavy[tid] = 0xFFFFFFFFu;
+    const bool heavy = tid < (int)ps.nuniq && ((ps.eq_mask[tid >> 5] >> (tid & 31)) & 1u);
+    const uint32_t nheavy = (uint32_t)__syncthreads_count(heavy);
+    uint32_t nmodel = NB - 2 * nheavy;
+    if (nmodel > (uint32_t)(2 * nb)) nmodel = 2 * nb;  // no more model buckets than the plain path aims for
+    if (nmodel < 2) nmodel = 2;
+    if (heavy) {
+        const K h = ps.uniq[tid];
+        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, h);
+        const uint32_t r = model_bucket<K>(leaf_p<K>(L.leaf[leaf_of<K>(p0)], h), nmodel);
+        atomicMin(&first_heavy[r], (uint32_t)tid);
+    }
+    __syncthreads();
+    L.heavy_flag[tid] = 0;
+    L.heavy[tid] = K(0);
+    if (first_heavy[tid] != 0xFFFFFFFFu && (uint32_t)tid < nmodel) {
+        L.heavy_flag[tid] = 1;
+        L.heavy[tid] = ps.uniq[first_heavy[tid]];
+    }
+    // bucket ids: a model bucket is one id, or three (below / equal / above)
+    // with a heavy key
+    const uint32_t width = (uint32_t)tid < nmodel ? (L.heavy_flag[tid] ? 3u : 1u) : 0u;
+    uint32_t tot_ids = 0;
+    const uint32_t id = block_exclusive_scan_first<NB, uint32_t>(width, wt32, &tot_ids);
+    L.base_id[tid] = (uint8_t)(id < NB ? id : NB - 1);
+    if (tid == 0) {
+        L.nmodel = nmodel;
+        L.nbuckets = tot_ids;
+    }
+    hist[tid] = 0;
+    __syncthreads();
+
+    // the sample through the model: its bucket histogram
     for (uint32_t i = tid; i < m; i += blockDim.x) atomicAdd(&hist[learned_bucket<K>(L, smp[i])], 1u);
     __syncthreads();
-    uint32_t c = tid < NB ? hist[tid] : 0u;
-    if (tid < NB && c) {
+    const uint32_t c = hist[tid];
+    if (c) {
         atomicMax(&max_s, c);
         atomicAdd(&nonempty_s, 1u);
     }
     // the "equal" bucket of each heavy model bucket r is base_id[r] + 1
     if (tid < NB / 32) L.bucket_eq[tid] = 0;
     __syncthreads();
-    if (tid < (int)nmodel && L.heavy_flag[tid]) {
+    if ((uint32_t)tid < nmodel && L.heavy_flag[tid]) {
         const uint32_t e = (uint32_t)L.base_id[tid] + 1;
         atomicOr(&L.bucket_eq[e >> 5], 1u << (e & 31));
     }
     const double scale = (double)sd.count / (double)m;
     uint64_t cap = 0;
-    if (tid < NB && (uint32_t)tid < L.nbuckets) {
+    if ((uint32_t)tid < L.nbuckets) {
         const double v = ((double)c + 6.0 * sqrt((double)c + 1.0) + 16.0) * scale;
         cap = (uint64_t)ceil(v);
         if (cap > sd.count) cap = sd.count;
         cap = (cap + 15) & ~15ull;
     }
     const uint64_t off = block_exclusive_scan_first<NB, uint64_t>(cap, wt64, (uint64_t*)nullptr);
-    if (tid < NB) {
-        L.region_off[tid] = off;
-        L.region_cap[tid] = cap;
+    L.region_off[tid] = off;
+    L.region_cap[tid] = cap;
+    // final loss of the whole model on the sample (root + leaves)
+    float lfs = 0.f;
+    for (uint32_t i = tid; i < m; i += blockDim.x) {
+        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, smp[i]);
+        const float r = leaf_p<K>(L.leaf[leaf_of<K>(p0)], smp[i]) - ((float)i + 0.5f) / (float)m;
+        lfs += r * r;
     }
+    atomicAdd(&loss_s, lfs / (float)m);
     __syncthreads();
     if (tid == 0) {
         const float mean = nonempty_s ? (float)m / (float)nonempty_s : 1.f;
         L.max_over_mean = (float)max_s / mean;
-        L.ok = (L.max_over_mean <= max_imbalance && L.nbuckets <= (uint32_t)NB) ? 1u : 0u;
-        // final loss of the whole model on the sample (root + leaves)
-        L.loss_final = 0.f;
+        L.balanced = (L.max_over_mean <= max_imbalance && L.nbuckets <= (uint32_t)NB) ? 1u : 0u;
+        L.ok = (L.balanced && L.searches) ? 1u : 0u;
+        L.loss_final = loss_s;
     }
     __syncthreads();
-    float lf = 0.f;
-    for (uint32_t i = tid; i < m; i += blockDim.x) {
-        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, smp[i]);
-        const float r = leaf_p<K>(L.leaf[leaf_of<K>(p0)], smp[i]) - ((float)i + 0.5f) / (float)m;
-        lf += r * r;
-    }
-    atomicAdd(&L.loss_final, lf / (float)m);
-    __syncthreads();
-    // copy out
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(&L);
     uint32_t* dst = reinterpret_cast<uint32_t*>(out + sgi);
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&L);
     for (uint32_t i = tid; i < sizeof(LearnedSet<K>) / 4; i += blockDim.x) dst[i] = src[i];
-    (void)wt32;
+}
+
+// The three launches of a fit (lfirst: nsegs * (LR_LEAVES + 1) words).
+// force: train every large segment, also where the table would not search
+// (the model is then reported but does not route).
+template <typename K>
+static void launch_learned_fit(const K* samples, const SegDesc* segs, uint32_t nsegs, const SplitSet<K>* plain,
+                               LearnedSet<K>* out, uint32_t* lfirst, int key_bytes, float max_imbalance,
+                               cudaStream_t st, int force = 0) {
+    learned_root_kernel<K><<<nsegs, LR_THREADS, 0, st>>>(samples, segs, nsegs, plain, out, lfirst, key_bytes,
+                                                         force);
+    learned_leaf_kernel<K><<<(nsegs * LR_LEAVES + 7) / 8, 256, 0, st>>>(samples, segs, nsegs, out, lfirst, key_bytes);
+    learned_finish_kernel<K><<<nsegs, NB, 0, st>>>(samples, segs, nsegs, plain, out, key_bytes, max_imbalance);
 }
 
 }  // namespace s512

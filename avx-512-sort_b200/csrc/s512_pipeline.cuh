@@ -202,10 +202,11 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     if (learned) {
         // the model is fitted to the same sorted sample; the split set above
         // stays as its fallback and supplies the heavy keys
-        learned_fit_kernel<K><<<nsegs, LR_THREADS, 0, st>>>(samples, L.segs, nsegs, splits, lsets, KB,
-                                                           (float)config().max_imbalance);
+        uint32_t* lfirst = (uint32_t*)C.get("lr_first", (size_t)nsegs * (LR_LEAVES + 1) * sizeof(uint32_t));
+        if (!lfirst) return S512_ERR_ALLOC;
+        launch_learned_fit<K>(samples, L.segs, nsegs, splits, lsets, lfirst, KB, (float)config().max_imbalance, st);
         S512_LAUNCH_CHECK();
-        S.kernel_launches += 1;
+        S.kernel_launches += 3;
         if (config().fault_inject & S512_FAULT_REJECT_MODEL) {
             inject_reject_kernel<K><<<1, 256, 0, st>>>(lsets, nsegs);
             S512_LAUNCH_CHECK();

@@ -454,15 +454,11 @@ namespace s512 {
 // Pipeline per block: the next tile travels into the second shared-memory
 // buffer by a 1-D bulk copy (TMA, completing on an mbarrier) while the
 // current one is ranked, staged and written; the buffer that held a tile's
-// raw keys is reused to stage them in bucket order.  Each bucket's run leaves
-// the stage by one 1-D bulk store (shared -> global), with the run placed in
-// the stage at the same 16-byte phase as its destination (up to PAD spare
-// keys per bucket) and its unaligned first and last keys stored by the
-// bucket's thread.  Three block barriers per tile: histogram complete | run
-// positions known | staging complete.  Two blocks share an SM, so one
-// block's barrier phases overlap the other's memory traffic.  When an input
-// array is not 16-byte aligned the tiles are read with plain loads instead
-// (a.tma == 0).
+// raw keys is reused to stage them in bucket order.  Three block barriers per
+// tile: histogram complete | bucket starts known | staging complete.  Two
+// blocks share an SM, so one block's barrier phases overlap the other's
+// memory traffic.  When an input array is not 16-byte aligned the tiles are
+// read with plain loads instead (a.tma == 0).
 constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in shared memory
 // Consecutive tiles a block claims at once: one segment's tables are loaded
 // once per group, so levels with many segments take longer runs; a single
@@ -508,15 +504,13 @@ constexpr size_t learned_model_bytes() { return offsetof(LearnedSet<K>, region_o
 template <typename K, int THREADS, int IPT>
 struct PartSmem {
     static constexpr int TILE = THREADS * IPT;
-    static constexpr int ALIGN_KEYS = 16 / (int)sizeof(K);  // keys per 16 bytes
-    static constexpr int PAD = ALIGN_KEYS - 1;              // spare keys per bucket run in the stage
-    alignas(128) unsigned char buf[2][(TILE + NB * PAD) * sizeof(K)];
+    alignas(128) unsigned char buf[2][TILE * sizeof(K)];
+    uint8_t bkt[TILE];
     uint64_t region_off[NB];
     uint64_t region_cap[NB];
-    uint64_t gofs[NB];            // destination of each bucket's run (GDELTA_DROP: none)
+    uint64_t gdelta[NB];
     uint32_t hist[NB];
-    uint32_t loc[NB];             // start of each bucket's run in the stage
-    uint32_t runlen[NB];
+    uint32_t loc[NB];
     uint32_t seg_tile_start[SEG_SMEM];
     uint64_t mbar[2];
     uint32_t tile_cur, has_eq, use_learned, abort;
@@ -739,16 +733,34 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 }
                 br[r] = bk | (rank << 8);
             }
-            // the previous tile's bulk stores have read their runs out of the
-            // buffer that thread 0 refills after the next barrier
-            if (tid < NB) bulk_wait_read_all();
             __syncthreads();  // (1) the tile's histogram is complete; the previous tile is written
 
-            // B. (warp 0) reserve the tile's share of each bucket's region,
-            // and place each bucket's run in the stage: an exclusive scan of
-            // (run + PAD), then the run's start moved up to the phase (mod 16
-            // bytes) of its destination.  Lane l owns buckets 8l .. 8l+7.
-            constexpr uint32_t AK = SM::ALIGN_KEYS;
+            // B. reserve the tile's share of each bucket's region, and the
+            // buckets' starts within the tile (exclusive scan by warp 0)
+            uint32_t h = 0;
+            unsigned long long off = 0;
+            if (tid < NB) {
+                h = sm.hist[tid];
+                if (h) off = atomicAdd(&a.fill[(size_t)seg * NB + tid], (unsigned long long)h);
+            }
+            if (tid < 32) {
+                uint32_t v[NB / 32];
+                uint32_t run = 0;
+#pragma unroll
+                for (int i = 0; i < NB / 32; ++i) {
+                    v[i] = run;
+                    run += sm.hist[tid * (NB / 32) + i];
+                }
+                uint32_t inc = run;
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+                    if (tid >= d) inc += o;
+                }
+                const uint32_t ex = inc - run;
+#pragma unroll
+                for (int i = 0; i < NB / 32; ++i) sm.loc[tid * (NB / 32) + i] = ex + v[i];
+            }
             if (tid == 0) {
                 // the next tile's keys into the other buffer: its last reader,
                 // the previous tile's write-out, finished before barrier (1)
@@ -756,55 +768,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 sm.tile_cur = t_next;
                 t_next = claim();
             }
-            if (tid < 32) {
-                constexpr int PB = NB / 32;
-                uint32_t hv[PB];
-                uint32_t sum = 0;
-#pragma unroll
-                for (int i = 0; i < PB; ++i) {
-                    hv[i] = sm.hist[tid * PB + i];
-                    sum += hv[i] + (uint32_t)SM::PAD;
-                }
-                // reservations four at a time; of each destination only its
-                // phase (2 bits) is kept for the placement below
-                uint32_t ph = 0;
-                const uint64_t obase = sm.sd.out_base;
-#pragma unroll
-                for (int q = 0; q < PB; q += 4) {
-                    unsigned long long ov[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        ov[j] = hv[q + j] ? atomicAdd(&a.fill[(size_t)seg * NB + tid * PB + q + j],
-                                                      (unsigned long long)hv[q + j])
-                                          : 0ull;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int bk = tid * PB + q + j;
-                        const uint64_t g = obase + sm.region_off[bk] + ov[j];
-                        const bool ovf = !data_ok || ov[j] + hv[q + j] > sm.region_cap[bk];
-                        if (ovf && hv[q + j]) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
-                        sm.gofs[bk] = ovf ? GDELTA_DROP : g;
-                        ph |= ((uint32_t)g & (AK - 1)) << (2 * (q + j));
-                    }
-                }
-                uint32_t inc = sum;
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-                    if (tid >= d) inc += o;
-                }
-                uint32_t locp = inc - sum;
-#pragma unroll
-                for (int i = 0; i < PB; ++i) {
-                    const int bk = tid * PB + i;
-                    sm.loc[bk] = locp + ((((ph >> (2 * i)) & 3u) - locp) & (AK - 1));
-                    sm.runlen[bk] = hv[i];
-                    sm.hist[bk] = 0;  // (next used after barrier (3))
-                    locp += hv[i] + (uint32_t)SM::PAD;
-                }
-            }
-            if (tid == 0 && !data_ok) sm.abort = 1;
-            __syncthreads();  // (2) run positions in the stage
+            __syncthreads();  // (2) bucket starts within the tile
 
             // C. stage the keys in bucket order, reusing this tile's buffer
             K* stage = reinterpret_cast<K*>(sm.buf[b]);
@@ -813,36 +777,35 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 const uint32_t idx = (uint32_t)(r * THREADS + tid);
                 if (FULL || idx < cnt) {
                     const uint32_t bk = br[r] & 0xFFu;
-                    stage[sm.loc[bk] + (br[r] >> 8)] = key[r];
+                    const uint32_t p = sm.loc[bk] + (br[r] >> 8);
+                    stage[p] = key[r];
+                    sm.bkt[p] = (uint8_t)bk;
                 }
             }
-            fence_proxy_async_smem();  // (the bulk stores read the stage)
+            if (tid < NB) {
+                const unsigned long long end = off + h;
+                const bool ovf = !data_ok || end > sm.region_cap[tid];
+                if (ovf && h) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
+                sm.gdelta[tid] =
+                    ovf ? GDELTA_DROP : sm.sd.out_base + sm.region_off[tid] + off - (uint64_t)sm.loc[tid];
+                sm.hist[tid] = 0;  // (next used after barrier (3))
+            }
+            if (tid == 0 && !data_ok) sm.abort = 1;
             __syncthreads();  // (3) staging complete
 
-            // D. write-out: thread b stores bucket b's run -- its unaligned
-            // first and last keys itself, the rest by one bulk store (an
-            // overflowed bucket's keys are dropped: the level is redone)
-            if (tid < NB) {
-                const uint32_t h = sm.runlen[tid];
-                const uint64_t g = sm.gofs[tid];
-                if (h && g != GDELTA_DROP) {
-                    const uint32_t s0 = sm.loc[tid];
-                    uint32_t head = (AK - (uint32_t)(g & (AK - 1))) & (AK - 1);
-                    head = head < h ? head : h;
-                    const uint32_t body = (h - head) & ~(AK - 1);
-                    for (uint32_t k = 0; k < head; ++k) a.out[g + k] = stage[s0 + k];
-                    if (body) {
-                        bulk_s2g(a.out + g + head, stage + s0 + head, body * (uint32_t)sizeof(K));
-                        bulk_commit();
-                    }
-                    for (uint32_t k = head + body; k < h; ++k) a.out[g + k] = stage[s0 + k];
+            // D. coalesced write-out (an overflowed bucket's keys are dropped:
+            // the level is redone)
+#pragma unroll
+            for (int r = 0; r < IPT; ++r) {
+                const uint32_t i = (uint32_t)(r * THREADS + tid);
+                if (FULL || i < cnt) {
+                    const uint64_t g = sm.gdelta[sm.bkt[i]];
+                    if (g != GDELTA_DROP) a.out[g + i] = stage[i];
                 }
             }
         }
         b ^= 1;
     }
-    // this thread's bulk stores complete before the block exits
-    if (tid < NB) bulk_wait_all();
     // after an abort, let a copy still in flight land before the block exits
     if (a.tma && sm.abort && tid == 0 && sm.tile_cur < ntiles) mbar_wait_bounded(&sm.mbar[b], (phases >> b) & 1u);
 }

@@ -232,7 +232,10 @@ typedef struct s512_learned_report {
     float loss_root;      /* root loss after training */
     float loss_final;     /* loss of root + leaves */
     float max_over_mean;  /* largest bucket / mean bucket, sample counts */
-    uint32_t nbuckets, nmodel, ok, pad_;
+    uint32_t nbuckets, nmodel;
+    uint32_t ok;          /* the model would route the segment: balanced, and the plain splitter table
+                             would search for many keys (clustered keys) */
+    uint32_t balanced;    /* max_over_mean within s512_config.max_imbalance */
 } s512_learned_report;
 S512_API int s512_learned_root_grad(int key_bytes, const void* d_sorted_keys, uint32_t m, const float* theta,
                                     float* loss, float* grad, void* stream);
