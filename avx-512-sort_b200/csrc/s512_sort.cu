@@ -87,6 +87,11 @@ int s512_sort_kv_i32(int* keys, int* values, size_t n, int flags, void* stream) 
     cudaStream_t st = (cudaStream_t)stream;
     S512_ENTER(C, st);
     S512_HOST_PTR(host, keys, flags);
+    if (host && stream_needed(n, 2 * sizeof(int))) {  // larger than the device budget
+        int rc = stream_sort_kv(*C, keys, values, n, st);
+        if (rc) return rc;
+        return finish_call(guard_, st, flags, host);
+    }
     int* dk = keys;
     int* dv = values;
     HostFeed feed;

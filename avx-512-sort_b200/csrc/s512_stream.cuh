@@ -2,8 +2,9 @@
 // sort streamed through the device in two passes over PCIe.
 //
 // The reference sorts host memory of any size in place (Sort512::Sort on a
-// host array; its benchmark goes to 2^30 keys, sort512perf.cpp:374).  A host
-// array whose sort would not fit the device budget (s512_config.device_budget,
+// host array; its benchmark goes to 2^30 keys, sort512perf.cpp:374; and
+// Sort512kv::Sort on two host arrays, sort512kv.hpp:6133).  A host array (or
+// key/value pair of arrays) whose sort would not fit the device budget (s512_config.device_budget,
 // about six times the data for the array plus the level buffers) is sorted
 // here as:
 //   1. runs: consecutive pieces of m keys are copied in, sorted on the device
@@ -36,21 +37,44 @@ inline uint64_t host_key(double x) {
     return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
 
+// How a streamed sort sees the caller's data: NARR host arrays of ESZ-byte
+// elements, the encoded key of element i, and the device codec of a piece.
 template <typename T> struct StreamTypes;
 template <> struct StreamTypes<int> {
     using K = uint32_t;
-    static CodecI32 codec(void* d) { return CodecI32{(const int*)d, (int*)d}; }
+    static constexpr int NARR = 1;
+    static constexpr size_t ESZ = 4;
+    static CodecI32 codec(void* const* d) { return CodecI32{(const int*)d[0], (int*)d[0]}; }
+    static uint64_t key(void* const* h, size_t i) { return host_key(static_cast<const int*>(h[0])[i]); }
 };
 template <> struct StreamTypes<double> {
     using K = uint64_t;
-    static CodecF64 codec(void* d) {
-        return CodecF64{(const unsigned long long*)d, (unsigned long long*)d};
+    static constexpr int NARR = 1;
+    static constexpr size_t ESZ = 8;
+    static CodecF64 codec(void* const* d) {
+        return CodecF64{(const unsigned long long*)d[0], (unsigned long long*)d[0]};
     }
+    static uint64_t key(void* const* h, size_t i) { return host_key(static_cast<const double*>(h[0])[i]); }
 };
 template <> struct StreamTypes<long long> {
     using K = uint64_t;
-    static CodecI64 codec(void* d) {
-        return CodecI64{(const unsigned long long*)d, (unsigned long long*)d};
+    static constexpr int NARR = 1;
+    static constexpr size_t ESZ = 8;
+    static CodecI64 codec(void* const* d) {
+        return CodecI64{(const unsigned long long*)d[0], (unsigned long long*)d[0]};
+    }
+    static uint64_t key(void* const* h, size_t i) { return host_key(static_cast<const long long*>(h[0])[i]); }
+};
+// int keys + int values in two arrays, ordered by (key, value) like the device codec
+struct StreamKV {
+    using K = uint64_t;
+    static constexpr int NARR = 2;
+    static constexpr size_t ESZ = 4;
+    static CodecKV codec(void* const* d) {
+        return CodecKV{(const int*)d[0], (const int*)d[1], (int*)d[0], (int*)d[1]};
+    }
+    static uint64_t key(void* const* h, size_t i) {
+        return (host_key(static_cast<const int*>(h[0])[i]) << 32) | host_key(static_cast<const int*>(h[1])[i]);
     }
 };
 
@@ -65,7 +89,8 @@ inline size_t device_budget() {
     return free_b / 10 * 8;
 }
 
-// Keys per streamed piece: the piece, its level buffers and scratch in ~6x.
+// Keys per streamed piece: the piece, its level buffers and scratch in ~6x
+// (esz: bytes of one element over all its arrays).
 inline size_t stream_piece_keys(size_t esz) {
     size_t m = device_budget() / (6 * esz);
     m &= ~(size_t)4095;
@@ -79,81 +104,88 @@ inline bool stream_needed(size_t n, size_t esz) {
     return n > stream_piece_keys(esz);
 }
 
-// Number of keys of the sorted run r[0..len) whose encoded key is <= v (or < v).
-template <typename T>
-static size_t count_le(const T* r, size_t len, uint64_t v, bool strict) {
+// Number of elements of the sorted run [first, first+len) of the staging
+// arrays whose encoded key is <= v (or < v).
+template <typename ST>
+static size_t count_le(void* const* stage, size_t first, size_t len, uint64_t v, bool strict) {
     size_t lo = 0, hi = len;
     while (lo < hi) {
         const size_t mid = lo + (hi - lo) / 2;
-        const uint64_t k = host_key(r[mid]);
+        const uint64_t k = ST::key(stage, first + mid);
         if (strict ? k < v : k <= v) lo = mid + 1; else hi = mid;
     }
     return lo;
 }
 
-template <typename T>
-static int stream_sort(DevCtx& C, T* host, size_t n, cudaStream_t st) {
-    using ST = StreamTypes<T>;
+template <typename ST>
+static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream_t st) {
     using K = typename ST::K;
-    const size_t esz = sizeof(T);
-    const size_t m = stream_piece_keys(esz);
+    constexpr int NA = ST::NARR;
+    const size_t esz = ST::ESZ;
+    const size_t m = stream_piece_keys(esz * NA);
     const size_t nruns = (n + m - 1) / m;
 
     struct Pinned {
-        T* p = nullptr;
+        void* p[2] = {nullptr, nullptr};
         ~Pinned() {
-            if (p) cudaFreeHost(p);
+            for (void* q : p)
+                if (q) cudaFreeHost(q);
         }
     } stage;
-    if (cudaMallocHost((void**)&stage.p, n * esz) != cudaSuccess) {
-        cudaGetLastError();
-        set_error("cudaMallocHost of %zu bytes for the streamed sort failed", n * esz);
-        return S512_ERR_ALLOC;
+    void* d[2] = {nullptr, nullptr};
+    for (int k = 0; k < NA; ++k) {
+        if (cudaMallocHost(&stage.p[k], n * esz) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMallocHost of %zu bytes for the streamed sort failed", n * esz);
+            return S512_ERR_ALLOC;
+        }
+        d[k] = C.get(k ? "stream_piece1" : "stream_piece0", m * esz);
+        if (!d[k]) return S512_ERR_ALLOC;
     }
-    T* d = (T*)C.get("stream_piece", m * esz);
-    if (!d) return S512_ERR_ALLOC;
+    auto at = [&](void* base, size_t i) { return static_cast<char*>(base) + i * esz; };
 
-    // 1. sorted runs of m keys into the staging array
+    // 1. sorted runs of m elements into the staging arrays
     for (size_t r = 0; r < nruns; ++r) {
         const size_t off = r * m, len = (n - off) < m ? (n - off) : m;
-        S512_CUDA_TRY(cudaMemcpyAsync(d, host + off, len * esz, cudaMemcpyHostToDevice, st));
+        for (int k = 0; k < NA; ++k)
+            S512_CUDA_TRY(cudaMemcpyAsync(d[k], at(host[k], off), len * esz, cudaMemcpyHostToDevice, st));
         int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
         if (rc) return rc;
-        S512_CUDA_TRY(cudaMemcpyAsync(stage.p + off, d, len * esz, cudaMemcpyDeviceToHost, st));
+        for (int k = 0; k < NA; ++k)
+            S512_CUDA_TRY(cudaMemcpyAsync(at(stage.p[k], off), d[k], len * esz, cudaMemcpyDeviceToHost, st));
     }
     S512_CUDA_TRY(cudaStreamSynchronize(st));
 
-    auto run_ptr = [&](size_t r) { return stage.p + r * m; };
     auto run_len = [&](size_t r) { return (n - r * m) < m ? (n - r * m) : m; };
 
-    // 2. cuts at ranks j*m: cut[j][r] = keys of run r that go before rank j*m
+    // 2. cuts at ranks j*m: cut[j][r] = elements of run r that go before rank j*m
     std::vector<std::vector<size_t>> cut(nruns + 1, std::vector<size_t>(nruns, 0));
     for (size_t r = 0; r < nruns; ++r) cut[nruns][r] = run_len(r);
     uint64_t kmin = ~0ull, kmax = 0;
     for (size_t r = 0; r < nruns; ++r) {
-        const uint64_t a = host_key(run_ptr(r)[0]), b = host_key(run_ptr(r)[run_len(r) - 1]);
+        const uint64_t a = ST::key(stage.p, r * m), b = ST::key(stage.p, r * m + run_len(r) - 1);
         kmin = a < kmin ? a : kmin;
         kmax = b > kmax ? b : kmax;
     }
     for (size_t j = 1; j < nruns; ++j) {
         const size_t rank = j * m;
-        // smallest encoded v with (keys <= v) >= rank
+        // smallest encoded v with (elements <= v) >= rank
         uint64_t lo = kmin, hi = kmax;
         while (lo < hi) {
             const uint64_t mid = lo + (hi - lo) / 2;
             size_t c = 0;
-            for (size_t r = 0; r < nruns; ++r) c += count_le(run_ptr(r), run_len(r), mid, false);
+            for (size_t r = 0; r < nruns; ++r) c += count_le<ST>(stage.p, r * m, run_len(r), mid, false);
             if (c >= rank) hi = mid; else lo = mid + 1;
         }
         const uint64_t v = lo;
         size_t below = 0;
         std::vector<size_t> lt(nruns), le(nruns);
         for (size_t r = 0; r < nruns; ++r) {
-            lt[r] = count_le(run_ptr(r), run_len(r), v, true);
-            le[r] = count_le(run_ptr(r), run_len(r), v, false);
+            lt[r] = count_le<ST>(stage.p, r * m, run_len(r), v, true);
+            le[r] = count_le<ST>(stage.p, r * m, run_len(r), v, false);
             below += lt[r];
         }
-        size_t need = rank - below;  // keys equal to v that go before the cut, taken in run order
+        size_t need = rank - below;  // elements equal to v that go before the cut, taken in run order
         for (size_t r = 0; r < nruns; ++r) {
             const size_t take = (le[r] - lt[r]) < need ? (le[r] - lt[r]) : need;
             cut[j][r] = lt[r] + take;
@@ -167,7 +199,9 @@ static int stream_sort(DevCtx& C, T* host, size_t n, cudaStream_t st) {
         for (size_t r = 0; r < nruns; ++r) {
             const size_t a = cut[j][r], b = cut[j + 1][r];
             if (b > a) {
-                S512_CUDA_TRY(cudaMemcpyAsync(d + len, run_ptr(r) + a, (b - a) * esz, cudaMemcpyHostToDevice, st));
+                for (int k = 0; k < NA; ++k)
+                    S512_CUDA_TRY(cudaMemcpyAsync(at(d[k], len), at(stage.p[k], r * m + a), (b - a) * esz,
+                                                  cudaMemcpyHostToDevice, st));
                 len += b - a;
             }
         }
@@ -177,10 +211,22 @@ static int stream_sort(DevCtx& C, T* host, size_t n, cudaStream_t st) {
         }
         int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
         if (rc) return rc;
-        S512_CUDA_TRY(cudaMemcpyAsync(host + j * m, d, len * esz, cudaMemcpyDeviceToHost, st));
+        for (int k = 0; k < NA; ++k)
+            S512_CUDA_TRY(cudaMemcpyAsync(at(host[k], j * m), d[k], len * esz, cudaMemcpyDeviceToHost, st));
     }
     S512_CUDA_TRY(cudaStreamSynchronize(st));
     return S512_OK;
+}
+
+template <typename T>
+static int stream_sort(DevCtx& C, T* host, size_t n, cudaStream_t st) {
+    void* h[1] = {host};
+    return stream_sort_arrays<StreamTypes<T>>(C, h, n, st);
+}
+
+static inline int stream_sort_kv(DevCtx& C, int* keys, int* values, size_t n, cudaStream_t st) {
+    void* h[2] = {keys, values};
+    return stream_sort_arrays<StreamKV>(C, h, n, st);
 }
 
 }  // namespace s512

@@ -64,3 +64,20 @@ def test_device_arrays_are_not_streamed(s512, cuda, small_budget):
     t = t0.clone()
     s512.sort(t)  # device memory: the budget concerns host arrays only
     assert torch.equal(t, torch.sort(t0).values)
+
+
+@pytest.mark.parametrize("distinct", [None, 17])
+def test_streamed_kv_pairs(distinct, s512, cuda, small_budget):
+    # Sort512kv::Sort on two host arrays past the budget: pairs end in
+    # (key, value) order, values travel with their keys
+    import workloads
+    n = (1 << 21) + 333
+    if distinct is None:
+        k = workloads.uniform_i32_np(n, 21)
+    else:  # ties across run boundaries, broken by the values
+        k = (workloads.uniform_i32_np(n, 21) % distinct).astype(np.int32)
+    v = workloads.uniform_i32_np(n, 22)
+    order = np.lexsort((v, k))
+    wk, wv = k[order], v[order]
+    s512.sort_kv(k, v)
+    assert np.array_equal(k, wk) and np.array_equal(v, wv)
