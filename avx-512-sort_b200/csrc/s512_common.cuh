@@ -282,10 +282,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
         : "memory");
     return ok != 0;
 }
+// try_wait that suspends the thread in hardware until the phase completes or
+// `ns` nanoseconds pass (instead of returning at once): a waiting warp takes
+// no issue slots from the other warps of the SM
+__device__ __forceinline__ bool mbar_try_wait_suspend(uint64_t* bar, uint32_t phase, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(phase), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+// Iterations of a suspending wait: at most about a second in all.
+constexpr uint32_t SUSPEND_NS = 1000;
+constexpr uint32_t SUSPEND_LIMIT = 1u << 20;
+
 // bounded wait for a phase of an mbarrier; false if the limit was reached
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t phase) {
-    for (uint32_t i = 0; i < SPIN_LIMIT; ++i)
-        if (mbar_try_wait(bar, phase)) return true;
+    for (uint32_t i = 0; i < SUSPEND_LIMIT; ++i)
+        if (mbar_try_wait_suspend(bar, phase, SUSPEND_NS)) return true;
     return false;
 }
 
