@@ -171,6 +171,7 @@ __device__ void root_forward_backward(const K* smp, uint32_t m, K kmin, float in
     // each thread walks a contiguous run of the (sorted) sample, so its
     // samples fall in few pieces: accumulate locally, flush on a piece change
     float lsum = 0.f;
+    const float inv_m = 1.f / (float)m;
     const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
     const uint32_t i0 = threadIdx.x * per;
     const uint32_t i1 = i0 + per < m ? i0 + per : m;
@@ -180,7 +181,7 @@ __device__ void root_forward_backward(const K* smp, uint32_t m, K kmin, float in
         float frac;
         int s;
         const float p0 = root_p0<K>(rc, rw, kmin, inv_range, smp[i], &frac, &s);
-        const float y = ((float)i + 0.5f) / (float)m;
+        const float y = ((float)i + 0.5f) * inv_m;
         const float r = p0 - y;
         lsum += r * r;
         if (s != cur) {
@@ -476,7 +477,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     __shared__ uint32_t first_heavy[NB];
     __shared__ uint32_t wt32[32];
     __shared__ uint64_t wt64[32];
-    __shared__ uint32_t max_s, nonempty_s;
+    __shared__ uint32_t max_s, nonempty_s, tot_ids_s;
     __shared__ float loss_s, top_w[NB / 32];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -542,12 +543,11 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     // bucket ids: a model bucket is one id, or three (below / equal / above)
     // with a heavy key
     const uint32_t width = (uint32_t)tid < nmodel ? (L.heavy_flag[tid] ? 3u : 1u) : 0u;
-    uint32_t tot_ids = 0;
-    const uint32_t id = block_exclusive_scan_first<NB, uint32_t>(width, wt32, &tot_ids);
+    const uint32_t id = block_exclusive_scan_first<NB, uint32_t>(width, wt32, &tot_ids_s);
     L.base_id[tid] = (uint8_t)(id < NB ? id : NB - 1);
     if (tid == 0) {
         L.nmodel = nmodel;
-        L.nbuckets = tot_ids;
+        L.nbuckets = tot_ids_s;  // (the scan's total, written by one thread to shared memory)
     }
     hist[tid] = 0;
     __syncthreads();
