@@ -199,11 +199,13 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     splitter_kernel<K><<<nsegs, NB, 0, st>>>(samples, L.segs, nsegs, splits, KB);
     S512_LAUNCH_CHECK();
     S.kernel_launches += 3;
+    int tfit0 = -1;
     if (learned) {
         // the model is fitted to the same sorted sample; the split set above
         // stays as its fallback and supplies the heavy keys
         uint32_t* lfirst = (uint32_t*)C.get("lr_first", (size_t)nsegs * (LR_LEAVES + 1) * sizeof(uint32_t));
         if (!lfirst) return S512_ERR_ALLOC;
+        tfit0 = tm.mark();
         launch_learned_fit<K>(samples, L.segs, nsegs, splits, lsets, lfirst, KB, (float)config().max_imbalance, st);
         S512_LAUNCH_CHECK();
         S.kernel_launches += 3;
@@ -345,8 +347,10 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     if (level < S512_MAX_LEVELS) {
         S.partition_keys[level] += (level == 0) ? (uint64_t)n : 0;
         S.partition_launches[level] += 1;
+        if (lsets) S.learned_segments[level] += host_ctl->learned_used;
         if (tm.on()) {
             S.sample_ms[level] += tm.ms(t0, t1);
+            if (tfit0 >= 0) S.fit_ms[level] += tm.ms(tfit0, t1);
             S.partition_ms[level] += tm.ms(t1, t2);
             S.leaf_ms[level] += tm.ms(t2, t4);
         }

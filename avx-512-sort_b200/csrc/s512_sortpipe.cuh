@@ -715,12 +715,21 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                                                  : (uint32_t)NB;
                 }
             }
+            // A warp whose 32 keys share a bucket (sorted or constant runs)
+            // ranks them with one atomic instead of 32 on one address.  Whether
+            // to look for that is decided once per tile from the warp's first
+            // 32 keys: on unsorted input the check would cost a shuffle and a
+            // vote per key and never pay.
+            const bool try_uni = __all_sync(0xFFFFFFFFu, bks[0] == __shfl_sync(0xFFFFFFFFu, bks[0], 0));
 #pragma unroll
             for (int r = 0; r < IPT; ++r) {
                 const uint32_t bk = bks[r];
-                // warp-uniform bucket (sorted / few-distinct input): one atomic for the warp
-                const uint32_t b0 = __shfl_sync(0xFFFFFFFFu, bk, 0);
-                const bool uni = __all_sync(0xFFFFFFFFu, bk == b0);
+                uint32_t b0 = bk;
+                bool uni = false;
+                if (try_uni) {
+                    b0 = __shfl_sync(0xFFFFFFFFu, bk, 0);
+                    uni = __all_sync(0xFFFFFFFFu, bk == b0);
+                }
                 uint32_t rank = 0;
                 if (uni) {
                     if (FULL || b0 < (uint32_t)NB) {

@@ -78,6 +78,8 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint32),
         ("key_bytes", ctypes.c_uint32),
         ("bucket_cv", ctypes.c_double * MAX_LEVELS),
+        ("fit_ms", ctypes.c_double * MAX_LEVELS),
+        ("learned_segments", ctypes.c_uint32 * MAX_LEVELS),
     ]
 
     def as_dict(self) -> dict:
@@ -97,6 +99,8 @@ class Stats(ctypes.Structure):
             "kernel_launches": int(self.kernel_launches),
             "key_bytes": int(self.key_bytes),
             "bucket_cv": list(self.bucket_cv[:lv]),
+            "fit_ms": list(self.fit_ms[:lv]),
+            "learned_segments": [int(x) for x in self.learned_segments[:lv]],
         }
 
 

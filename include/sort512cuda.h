@@ -109,6 +109,8 @@ typedef struct s512_stats {
     uint32_t kernel_launches;               /* kernels launched by the call */
     uint32_t key_bytes;                     /* 4 or 8 */
     double bucket_cv[S512_MAX_LEVELS];      /* std / mean of the non-empty bucket sizes, per level */
+    double fit_ms[S512_MAX_LEVELS];         /* learned model fit (part of sample_ms), per level */
+    uint32_t learned_segments[S512_MAX_LEVELS]; /* segments routed by their learned model, per level */
 } s512_stats;
 
 /* --- configuration, errors, resources ---------------------------------- */
