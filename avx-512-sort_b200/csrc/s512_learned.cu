@@ -9,23 +9,20 @@ namespace s512 {
 template <typename K>
 __global__ void __launch_bounds__(LR_THREADS) root_grad_kernel(const K* __restrict__ smp, uint32_t m,
                                                                const float* __restrict__ theta, float* __restrict__ out) {
-    __shared__ float rw[LR_ROOT], rc[LR_ROOT], S0[LR_ROOT], S1[LR_ROOT], gw[LR_ROOT];
-    __shared__ float loss;
-    if (threadIdx.x < LR_ROOT) rw[threadIdx.x] = theta[threadIdx.x] * theta[threadIdx.x];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float c = 0.f;
-        for (int t = 0; t < LR_ROOT; ++t) {
-            rc[t] = c;
-            c += rw[t];
-        }
-    }
-    __syncthreads();
+    __shared__ double mom[LR_ROOT][RM_COUNT];
+    __shared__ uint32_t pstart[LR_ROOT + 1];
     const K kmin = smp[0], range = smp[m - 1] - smp[0];
     const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
-    root_forward_backward<K>(smp, m, kmin, inv_range, rc, rw, S0, S1, &loss, gw);
-    if (threadIdx.x < LR_ROOT) out[1 + threadIdx.x] = gw[threadIdx.x] * 2.f * theta[threadIdx.x];
-    if (threadIdx.x == 0) out[0] = loss;
+    root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
+    if (threadIdx.x < 32) {
+        const int l = threadIdx.x;
+        const float th0 = theta[2 * l], th1 = theta[2 * l + 1];
+        double loss, g0, g1;
+        root_eval_warp(mom, m, th0, th1, &loss, &g0, &g1);
+        out[1 + 2 * l] = (float)(g0 * 2.0 * th0);
+        out[2 + 2 * l] = (float)(g1 * 2.0 * th1);
+        if (l == 0) out[0] = (float)loss;
+    }
 }
 
 template <typename K>

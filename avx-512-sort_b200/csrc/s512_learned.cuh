@@ -25,6 +25,8 @@
 // theta with the analytic gradient
 //   dL/dw_t = (2/m) * ( sum_{i: s_i > t} r_i + sum_{i: s_i = t} r_i * frac_i ),
 //   dL/dtheta_t = dL/dw_t * 2 * theta_t,         r_i = p0(z_i) - y_i.
+// Both sums are evaluated from six per-piece sums of the sample taken once
+// (root_moments below), so the steps themselves never touch the sample.
 // Each leaf starts from its least-squares line on the samples routed to it,
 // which is already the optimum of its squared error when its slope is
 // positive; a leaf whose least-squares slope was clipped to 0 takes
@@ -94,16 +96,22 @@ struct LearnedSet {
 __device__ __forceinline__ float key_to_float(uint32_t d) { return __uint2float_rn(d); }
 __device__ __forceinline__ float key_to_float(uint64_t d) { return __ull2float_rn(d); }
 
+// The root piece of a key (pieces split [kmin, kmin + range] evenly) and its
+// place inside the piece, in [0, 1].
 template <typename K>
-__device__ __forceinline__ float root_p0(const float* rc, const float* rw, K kmin, float inv_range, K key,
-                                         float* frac_out = nullptr, int* seg_out = nullptr) {
+__device__ __forceinline__ int root_piece(K kmin, float inv_range, K key, float* frac) {
     const K d = key > kmin ? key - kmin : K(0);
     const float zr = key_to_float(d) * inv_range * (float)LR_ROOT;
     int s = (int)zr;
     s = s < 0 ? 0 : (s > LR_ROOT - 1 ? LR_ROOT - 1 : s);
-    const float frac = zr - (float)s;
-    if (frac_out) *frac_out = frac;
-    if (seg_out) *seg_out = s;
+    *frac = zr - (float)s;
+    return s;
+}
+
+template <typename K>
+__device__ __forceinline__ float root_p0(const float* rc, const float* rw, K kmin, float inv_range, K key) {
+    float frac;
+    const int s = root_piece<K>(kmin, inv_range, key, &frac);
     return rc[s] + rw[s] * frac;
 }
 
@@ -156,60 +164,97 @@ struct Adam {
     }
 };
 
-// Root forward + backward over the sorted sample: loss, and dL/dw per piece.
-// rc/rw are the un-normalised running sums / slopes.  Block-wide; S0/S1 and
-// loss_acc are shared scratch.
+// The root's training data, gathered once.  A sample's piece s_i and its
+// place f_i inside the piece depend on its key only (not on theta), so with
+// p0_i = rc[s_i] + rw[s_i] * f_i, y_i = (i + 1/2) / m and r_i = p0_i - y_i,
+// the loss (1/m) sum r_i^2 and the per-piece sums S0_t = sum r_i,
+// S1_t = sum r_i f_i (over the samples of piece t) are quadratic in
+// (rc_t, rw_t) with six fixed coefficients per piece:
+//   n_t, sum f, sum f^2, sum y, sum y^2, sum y f.
+// One pass over the sample collects them (in double: the loss is a small
+// difference of these sums); a training step is then O(pieces) work in one
+// warp.
+constexpr int RM_N = 0, RM_F = 1, RM_FF = 2, RM_Y = 3, RM_YY = 4, RM_YF = 5, RM_COUNT = 6;
+
+// Block-wide.  pstart[t] (LR_ROOT + 1 entries) receives the first sample of
+// piece t (samples are sorted and the piece is monotone in the key).
 template <typename K>
-__device__ void root_forward_backward(const K* smp, uint32_t m, K kmin, float inv_range, const float* rc,
-                                      const float* rw, float* S0, float* S1, float* loss_acc, float* gw) {
-    for (int t = threadIdx.x; t < LR_ROOT; t += blockDim.x) {
-        S0[t] = 0.f;
-        S1[t] = 0.f;
-    }
-    if (threadIdx.x == 0) *loss_acc = 0.f;
+__device__ void root_moments(const K* smp, uint32_t m, K kmin, float inv_range, uint32_t* pstart,
+                             double (*mom)[RM_COUNT]) {
+    const int tid = threadIdx.x;
+    for (int t = tid; t <= LR_ROOT; t += blockDim.x) pstart[t] = m;
     __syncthreads();
-    // each thread walks a contiguous run of the (sorted) sample, so its
-    // samples fall in few pieces: accumulate locally, flush on a piece change
-    float lsum = 0.f;
-    const float inv_m = 1.f / (float)m;
-    const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
-    const uint32_t i0 = threadIdx.x * per;
-    const uint32_t i1 = i0 + per < m ? i0 + per : m;
-    int cur = -1;
-    float a0 = 0.f, a1 = 0.f;
-    for (uint32_t i = i0; i < i1; ++i) {
-        float frac;
-        int s;
-        const float p0 = root_p0<K>(rc, rw, kmin, inv_range, smp[i], &frac, &s);
-        const float y = ((float)i + 0.5f) * inv_m;
-        const float r = p0 - y;
-        lsum += r * r;
-        if (s != cur) {
-            if (cur >= 0) {
-                atomicAdd(&S0[cur], a0);
-                atomicAdd(&S1[cur], a1);
-            }
-            cur = s;
-            a0 = a1 = 0.f;
+    for (uint32_t i = tid; i < m; i += blockDim.x) {
+        float f;
+        const int s = root_piece<K>(kmin, inv_range, smp[i], &f);
+        const int sp = i == 0 ? -1 : root_piece<K>(kmin, inv_range, smp[i - 1], &f);
+        for (int q = sp + 1; q <= s; ++q) pstart[q] = i;
+    }
+    __syncthreads();
+    const int lane = tid & 31, nw = blockDim.x >> 5;
+    const double inv_m = 1.0 / (double)m;
+    for (int t = tid >> 5; t < LR_ROOT; t += nw) {
+        double a[RM_COUNT] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (uint32_t i = pstart[t] + lane; i < pstart[t + 1]; i += 32) {
+            float ff;
+            (void)root_piece<K>(kmin, inv_range, smp[i], &ff);
+            const double f = (double)ff, y = ((double)i + 0.5) * inv_m;
+            a[RM_N] += 1.0;
+            a[RM_F] += f;
+            a[RM_FF] += f * f;
+            a[RM_Y] += y;
+            a[RM_YY] += y * y;
+            a[RM_YF] += y * f;
         }
-        a0 += r;
-        a1 += r * frac;
-    }
-    if (cur >= 0) {
-        atomicAdd(&S0[cur], a0);
-        atomicAdd(&S1[cur], a1);
-    }
-    atomicAdd(loss_acc, lsum);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float suffix = 0.f;  // sum of r over later pieces
-        for (int t = LR_ROOT - 1; t >= 0; --t) {
-            gw[t] = 2.f / (float)m * (suffix + S1[t]);
-            suffix += S0[t];
+#pragma unroll
+        for (int k = 0; k < RM_COUNT; ++k) {
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) a[k] += __shfl_xor_sync(0xFFFFFFFFu, a[k], d);
         }
-        *loss_acc /= (float)m;
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < RM_COUNT; ++k) mom[t][k] = a[k];
     }
     __syncthreads();
+}
+
+// One warp, two pieces a lane (2*lane, 2*lane + 1): the loss of the root with
+// w_t = theta_t^2 (rw = w, rc = exclusive running sum of w) and dL/dw_t,
+//   dL/dw_t = (2/m) * (S1_t + sum_{u > t} S0_u).
+__device__ __forceinline__ void root_eval_warp(const double (*mom)[RM_COUNT], uint32_t m, float th0, float th1,
+                                               double* loss, double* g0, double* g1) {
+    const int lane = threadIdx.x & 31;
+    const double w0 = (double)th0 * th0, w1 = (double)th1 * th1;
+    double inc = w0 + w1;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+        if (lane >= d) inc += o;
+    }
+    const double rc0 = inc - (w0 + w1), rc1 = rc0 + w0;
+    auto piece = [](const double* M, double A, double B, double* S0, double* S1) -> double {
+        *S0 = M[RM_N] * A + B * M[RM_F] - M[RM_Y];
+        *S1 = A * M[RM_F] + B * M[RM_FF] - M[RM_YF];
+        return M[RM_N] * A * A + B * B * M[RM_FF] + M[RM_YY] + 2.0 * A * B * M[RM_F] - 2.0 * A * M[RM_Y] -
+               2.0 * B * M[RM_YF];
+    };
+    double s00, s10, s01, s11;
+    double l = piece(mom[2 * lane], rc0, w0, &s00, &s10) + piece(mom[2 * lane + 1], rc1, w1, &s01, &s11);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) l += __shfl_xor_sync(0xFFFFFFFFu, l, d);
+    // S0 summed over the pieces after each of this lane's two
+    double pre = s00 + s01;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const double o = __shfl_up_sync(0xFFFFFFFFu, pre, d);
+        if (lane >= d) pre += o;
+    }
+    const double total = __shfl_sync(0xFFFFFFFFu, pre, 31);
+    const double after1 = total - pre, after0 = after1 + s01;
+    const double k = 2.0 / (double)m;
+    *g0 = k * (after0 + s10);
+    *g1 = k * (after1 + s11);
+    *loss = (l > 0.0 ? l : 0.0) / (double)m;
 }
 
 // --- fit, launch 1: the root of each segment (one block of LR_THREADS each).
@@ -225,8 +270,10 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
                                                                   int force) {
     const uint32_t sgi = blockIdx.x;
     if (sgi >= nsegs) return;
-    __shared__ float theta[LR_ROOT], rw[LR_ROOT], rc[LR_ROOT], gw[LR_ROOT], S0[LR_ROOT], S1[LR_ROOT];
-    __shared__ float loss_acc, loss_init_s;
+    __shared__ double mom[LR_ROOT][RM_COUNT];
+    __shared__ uint32_t pstart[LR_ROOT + 1];
+    __shared__ float rw[LR_ROOT];
+    __shared__ float loss_init_s, loss_best_s;
     __shared__ uint32_t search_s;
     const SegDesc sd = segs[sgi];
     const int tid = threadIdx.x;
@@ -266,71 +313,40 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
     const K range = kmax - kmin;
     const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
 
-    // root init: histogram of the sample over the pieces, theta = sqrt(w)
-    for (int t = tid; t < LR_ROOT; t += blockDim.x) S0[t] = 0.f;
-    __syncthreads();
-    {
-        const uint32_t per = (m + blockDim.x - 1) / blockDim.x;
-        const uint32_t i0 = tid * per;
-        const uint32_t i1 = i0 + per < m ? i0 + per : m;
-        int cur = -1;
-        float acc = 0.f;
-        for (uint32_t i = i0; i < i1; ++i) {
-            const K d = smp[i] > kmin ? smp[i] - kmin : K(0);
-            const float zr = key_to_float(d) * inv_range * (float)LR_ROOT;
-            int s = (int)zr;
-            s = s < 0 ? 0 : (s > LR_ROOT - 1 ? LR_ROOT - 1 : s);
-            if (s != cur) {
-                if (cur >= 0) atomicAdd(&S0[cur], acc);
-                cur = s;
-                acc = 0.f;
-            }
-            acc += 1.f / (float)m;
-        }
-        if (cur >= 0) atomicAdd(&S0[cur], acc);
-    }
-    __syncthreads();
-    if (tid < LR_ROOT) theta[tid] = sqrtf(S0[tid]);
-    __syncthreads();
-
-    // Adam on theta; the parameters with the lowest loss seen are kept, so
-    // training never ends worse than the histogram start
+    // the training data (per-piece sums), then Adam on theta in warp 0, two
+    // pieces a lane, from the histogram start theta = sqrt(n_t / m); the
+    // parameters with the lowest loss seen are kept, so training never ends
+    // worse than its start
+    root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
     static_assert(LR_ROOT == 64, "two root pieces per lane of warp 0");
-    Adam opt;
-    float best_theta = tid < LR_ROOT ? theta[tid] : 0.f;
-    float best_loss = 3.4e38f;
-    for (int it = 0; it <= LR_ITERS; ++it) {
-        // slopes and their running sums (rc) by warp 0, two pieces a lane
-        if (tid < 32) {
-            const float w0 = theta[2 * tid] * theta[2 * tid], w1 = theta[2 * tid + 1] * theta[2 * tid + 1];
-            float inc = w0 + w1;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-                const float o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
-                if (tid >= d) inc += o;
+    if (tid < 32) {
+        float th0 = sqrtf((float)(mom[2 * tid][RM_N] / (double)m));
+        float th1 = sqrtf((float)(mom[2 * tid + 1][RM_N] / (double)m));
+        float b0 = th0, b1 = th1;
+        double best = 1e300, first = 0.0;
+        Adam o0, o1;
+        for (int it = 0; it <= LR_ITERS; ++it) {
+            double loss, g0, g1;
+            root_eval_warp(mom, m, th0, th1, &loss, &g0, &g1);
+            if (it == 0) first = loss;
+            if (loss < best) {
+                best = loss;
+                b0 = th0;
+                b1 = th1;
             }
-            const float ex = inc - (w0 + w1);
-            rw[2 * tid] = w0;
-            rw[2 * tid + 1] = w1;
-            rc[2 * tid] = ex;
-            rc[2 * tid + 1] = ex + w0;
+            if (it == LR_ITERS) break;
+            th0 -= o0.step((float)(g0 * 2.0 * th0), LR_STEP * 0.125f, it + 1);
+            th1 -= o1.step((float)(g1 * 2.0 * th1), LR_STEP * 0.125f, it + 1);
         }
-        __syncthreads();
-        root_forward_backward<K>(smp, m, kmin, inv_range, rc, rw, S0, S1, &loss_acc, gw);
-        const float loss = loss_acc;
-        if (it == 0 && tid == 0) loss_init_s = loss;
-        if (loss < best_loss) {
-            best_loss = loss;
-            if (tid < LR_ROOT) best_theta = theta[tid];
+        rw[2 * tid] = b0 * b0;
+        rw[2 * tid + 1] = b1 * b1;
+        if (tid == 0) {
+            loss_init_s = (float)first;
+            loss_best_s = (float)best;
         }
-        if (it == LR_ITERS) break;
-        if (tid < LR_ROOT) theta[tid] -= opt.step(gw[tid] * 2.f * theta[tid], LR_STEP * 0.125f, it + 1);
-        __syncthreads();
     }
     __syncthreads();
     // the kept root, normalised so that it spans [0, 1]
-    if (tid < LR_ROOT) rw[tid] = best_theta * best_theta;
-    __syncthreads();
     if (tid == 0) {
         float tot = 0.f;
         for (int t = 0; t < LR_ROOT; ++t) tot += rw[t];
@@ -344,7 +360,7 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
         L.kmin = kmin;
         L.inv_range = inv_range;
         L.loss_init = loss_init_s;
-        L.loss_root = best_loss;
+        L.loss_root = loss_best_s;
         L.fitted = 1;
         L.searches = searches ? 1u : 0u;
     }

@@ -347,7 +347,13 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     if (level < S512_MAX_LEVELS) {
         S.partition_keys[level] += (level == 0) ? (uint64_t)n : 0;
         S.partition_launches[level] += 1;
-        if (lsets) S.learned_segments[level] += host_ctl->learned_used;
+        if (lsets) {
+            S.learned_segments[level] += host_ctl->learned_used;
+            S.learned_fitted[level] += host_ctl->learned_fitted;
+            float imb;
+            memcpy(&imb, &host_ctl->model_imb_bits, sizeof(imb));
+            if (host_ctl->learned_fitted && imb > S.model_max_over_mean[level]) S.model_max_over_mean[level] = imb;
+        }
         if (tm.on()) {
             S.sample_ms[level] += tm.ms(t0, t1);
             if (tfit0 >= 0) S.fit_ms[level] += tm.ms(tfit0, t1);

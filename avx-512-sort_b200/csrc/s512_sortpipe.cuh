@@ -142,6 +142,8 @@ struct LevelCtl {
     uint64_t level_keys;      // keys partitioned this level
     uint32_t learned_used;    // segments routed by their learned model
     uint32_t plain_used;      // segments routed by the splitter tree
+    uint32_t learned_fitted;  // segments whose learned model was trained
+    uint32_t model_imb_bits;  // largest sample imbalance of a trained model (float bits)
     uint32_t n_uneven[NCLASS];  // leaves handed from the slot sort to the block sort
     uint32_t never_set;       // testing: a flag nothing writes (the injected wait)
     double bucket_sq;         // sum of squared non-empty bucket sizes this level
@@ -918,7 +920,13 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
     const uint64_t* region_off = use_learned ? a.learned[s].region_off : a.splits[s].region_off;
     const uint32_t* bucket_eq = use_learned ? a.learned[s].bucket_eq : a.splits[s].bucket_eq;
     const int b = threadIdx.x;
-    if (b == 0) atomicAdd(use_learned ? &a.ctl->learned_used : &a.ctl->plain_used, 1u);
+    if (b == 0) {
+        atomicAdd(use_learned ? &a.ctl->learned_used : &a.ctl->plain_used, 1u);
+        if (a.learned && a.learned[s].fitted) {
+            atomicAdd(&a.ctl->learned_fitted, 1u);
+            atomicMax(&a.ctl->model_imb_bits, __float_as_uint(a.learned[s].max_over_mean));  // (>= 0)
+        }
+    }
     const uint64_t c = (b < (int)nbk) ? a.bucket_counts[(size_t)s * NB + b] : 0ull;
     const uint64_t excl = block_exclusive_scan_first<NB, uint64_t>(c, wtot64, (uint64_t*)nullptr);
     if (c == 0) return;

@@ -80,6 +80,8 @@ class Stats(ctypes.Structure):
         ("bucket_cv", ctypes.c_double * MAX_LEVELS),
         ("fit_ms", ctypes.c_double * MAX_LEVELS),
         ("learned_segments", ctypes.c_uint32 * MAX_LEVELS),
+        ("learned_fitted", ctypes.c_uint32 * MAX_LEVELS),
+        ("model_max_over_mean", ctypes.c_double * MAX_LEVELS),
     ]
 
     def as_dict(self) -> dict:
@@ -101,6 +103,8 @@ class Stats(ctypes.Structure):
             "bucket_cv": list(self.bucket_cv[:lv]),
             "fit_ms": list(self.fit_ms[:lv]),
             "learned_segments": [int(x) for x in self.learned_segments[:lv]],
+            "learned_fitted": [int(x) for x in self.learned_fitted[:lv]],
+            "model_max_over_mean": list(self.model_max_over_mean[:lv]),
         }
 
 

@@ -111,6 +111,8 @@ typedef struct s512_stats {
     double bucket_cv[S512_MAX_LEVELS];      /* std / mean of the non-empty bucket sizes, per level */
     double fit_ms[S512_MAX_LEVELS];         /* learned model fit (part of sample_ms), per level */
     uint32_t learned_segments[S512_MAX_LEVELS]; /* segments routed by their learned model, per level */
+    uint32_t learned_fitted[S512_MAX_LEVELS];   /* segments whose model was trained, per level */
+    double model_max_over_mean[S512_MAX_LEVELS]; /* worst sample imbalance of a trained model, per level */
 } s512_stats;
 
 /* --- configuration, errors, resources ---------------------------------- */
