@@ -16,11 +16,13 @@ __global__ void __launch_bounds__(LR_THREADS) root_grad_kernel(const K* __restri
     root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
-        const float th0 = theta[2 * l], th1 = theta[2 * l + 1];
-        double loss, g0, g1;
-        root_eval_warp(mom, m, th0, th1, &loss, &g0, &g1);
-        out[1 + 2 * l] = (float)(g0 * 2.0 * th0);
-        out[2 + 2 * l] = (float)(g1 * 2.0 * th1);
+        float th[RP];
+#pragma unroll
+        for (int k = 0; k < RP; ++k) th[k] = theta[l * RP + k];
+        double loss, g[RP];
+        root_eval_warp(mom, m, th, &loss, g);
+#pragma unroll
+        for (int k = 0; k < RP; ++k) out[1 + l * RP + k] = (float)(g[k] * 2.0 * th[k]);
         if (l == 0) out[0] = (float)loss;
     }
 }

@@ -48,9 +48,10 @@
 namespace s512 {
 
 // Segments below this many keys are not fitted: a partition pass over them
-// is short next to the fit (the levels with thousands of small segments).
-constexpr uint64_t LR_MIN_KEYS = 1ull << 19;
-constexpr int LR_ROOT = 64;
+// is short next to the fit, and once the first level has split the clusters
+// apart the splitter table rarely searches (the levels of many segments).
+constexpr uint64_t LR_MIN_KEYS = 1ull << 23;
+constexpr int LR_ROOT = 256;
 constexpr int LR_LEAVES = 256;
 constexpr int LR_THREADS = 512;
 constexpr int LR_ITERS = 16;
@@ -87,7 +88,7 @@ struct LearnedSet {
     uint32_t fitted;     // 1: trained (0: too small, or the splitter table needs no searches)
     uint32_t searches;   // 1: the splitter table would search for many of the segment's keys
     float loss_init, loss_root, loss_final;
-    float max_over_mean;  // sample-count imbalance of the learned buckets
+    float max_over_mean;  // sample-count imbalance of the learned buckets (equal buckets aside)
 };
 
 // ---------------------------------------------------------------------------
@@ -218,42 +219,56 @@ __device__ void root_moments(const K* smp, uint32_t m, K kmin, float inv_range, 
     __syncthreads();
 }
 
-// One warp, two pieces a lane (2*lane, 2*lane + 1): the loss of the root with
-// w_t = theta_t^2 (rw = w, rc = exclusive running sum of w) and dL/dw_t,
+// One warp, RP = LR_ROOT / 32 consecutive pieces a lane (lane * RP + k): the
+// loss of the root with w_t = theta_t^2 (rw = w, rc = exclusive running sum
+// of w) and dL/dw_t,
 //   dL/dw_t = (2/m) * (S1_t + sum_{u > t} S0_u).
-__device__ __forceinline__ void root_eval_warp(const double (*mom)[RM_COUNT], uint32_t m, float th0, float th1,
-                                               double* loss, double* g0, double* g1) {
+constexpr int RP = LR_ROOT / 32;
+__device__ __forceinline__ void root_eval_warp(const double (*mom)[RM_COUNT], uint32_t m, const float (&th)[RP],
+                                               double* loss, double (&g)[RP]) {
     const int lane = threadIdx.x & 31;
-    const double w0 = (double)th0 * th0, w1 = (double)th1 * th1;
-    double inc = w0 + w1;
+    double w[RP], lane_w = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+        w[k] = (double)th[k] * th[k];
+        lane_w += w[k];
+    }
+    double inc = lane_w;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const double o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
         if (lane >= d) inc += o;
     }
-    const double rc0 = inc - (w0 + w1), rc1 = rc0 + w0;
-    auto piece = [](const double* M, double A, double B, double* S0, double* S1) -> double {
-        *S0 = M[RM_N] * A + B * M[RM_F] - M[RM_Y];
-        *S1 = A * M[RM_F] + B * M[RM_FF] - M[RM_YF];
-        return M[RM_N] * A * A + B * B * M[RM_FF] + M[RM_YY] + 2.0 * A * B * M[RM_F] - 2.0 * A * M[RM_Y] -
-               2.0 * B * M[RM_YF];
-    };
-    double s00, s10, s01, s11;
-    double l = piece(mom[2 * lane], rc0, w0, &s00, &s10) + piece(mom[2 * lane + 1], rc1, w1, &s01, &s11);
+    double rc = inc - lane_w;  // running sum before this lane's first piece
+    double S0[RP], S1[RP], l = 0.0, lane_s0 = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP; ++k) {
+        const double* M = mom[lane * RP + k];
+        const double A = rc, B = w[k];
+        S0[k] = M[RM_N] * A + B * M[RM_F] - M[RM_Y];
+        S1[k] = A * M[RM_F] + B * M[RM_FF] - M[RM_YF];
+        l += M[RM_N] * A * A + B * B * M[RM_FF] + M[RM_YY] + 2.0 * A * B * M[RM_F] - 2.0 * A * M[RM_Y] -
+             2.0 * B * M[RM_YF];
+        lane_s0 += S0[k];
+        rc += w[k];
+    }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) l += __shfl_xor_sync(0xFFFFFFFFu, l, d);
-    // S0 summed over the pieces after each of this lane's two
-    double pre = s00 + s01;
+    // S0 summed over the pieces after each piece: the later lanes' totals,
+    // then this lane's later pieces
+    double pre = lane_s0;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const double o = __shfl_up_sync(0xFFFFFFFFu, pre, d);
         if (lane >= d) pre += o;
     }
-    const double total = __shfl_sync(0xFFFFFFFFu, pre, 31);
-    const double after1 = total - pre, after0 = after1 + s01;
-    const double k = 2.0 / (double)m;
-    *g0 = k * (after0 + s10);
-    *g1 = k * (after1 + s11);
+    double after = __shfl_sync(0xFFFFFFFFu, pre, 31) - pre;
+    const double kk = 2.0 / (double)m;
+#pragma unroll
+    for (int k = RP - 1; k >= 0; --k) {
+        g[k] = kk * (after + S1[k]);
+        after += S0[k];
+    }
     *loss = (l > 0.0 ? l : 0.0) / (double)m;
 }
 
@@ -318,28 +333,28 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
     // parameters with the lowest loss seen are kept, so training never ends
     // worse than its start
     root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
-    static_assert(LR_ROOT == 64, "two root pieces per lane of warp 0");
+    static_assert(LR_ROOT % 32 == 0, "whole pieces per lane of warp 0");
     if (tid < 32) {
-        float th0 = sqrtf((float)(mom[2 * tid][RM_N] / (double)m));
-        float th1 = sqrtf((float)(mom[2 * tid + 1][RM_N] / (double)m));
-        float b0 = th0, b1 = th1;
+        float th[RP], best_th[RP];
+        Adam opt[RP];
+#pragma unroll
+        for (int k = 0; k < RP; ++k) best_th[k] = th[k] = sqrtf((float)(mom[tid * RP + k][RM_N] / (double)m));
         double best = 1e300, first = 0.0;
-        Adam o0, o1;
         for (int it = 0; it <= LR_ITERS; ++it) {
-            double loss, g0, g1;
-            root_eval_warp(mom, m, th0, th1, &loss, &g0, &g1);
+            double loss, g[RP];
+            root_eval_warp(mom, m, th, &loss, g);
             if (it == 0) first = loss;
             if (loss < best) {
                 best = loss;
-                b0 = th0;
-                b1 = th1;
+#pragma unroll
+                for (int k = 0; k < RP; ++k) best_th[k] = th[k];
             }
             if (it == LR_ITERS) break;
-            th0 -= o0.step((float)(g0 * 2.0 * th0), LR_STEP * 0.125f, it + 1);
-            th1 -= o1.step((float)(g1 * 2.0 * th1), LR_STEP * 0.125f, it + 1);
+#pragma unroll
+            for (int k = 0; k < RP; ++k) th[k] -= opt[k].step((float)(g[k] * 2.0 * th[k]), LR_STEP * 0.125f, it + 1);
         }
-        rw[2 * tid] = b0 * b0;
-        rw[2 * tid + 1] = b1 * b1;
+#pragma unroll
+        for (int k = 0; k < RP; ++k) rw[tid * RP + k] = best_th[k] * best_th[k];
         if (tid == 0) {
             loss_init_s = (float)first;
             loss_best_s = (float)best;
@@ -493,7 +508,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     __shared__ uint32_t first_heavy[NB];
     __shared__ uint32_t wt32[32];
     __shared__ uint64_t wt64[32];
-    __shared__ uint32_t max_s, nonempty_s, tot_ids_s;
+    __shared__ uint32_t max_s, nonempty_s, tot_ids_s, sorted_s;
     __shared__ float loss_s, top_w[NB / 32];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -508,6 +523,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     if (tid == 0) {
         max_s = 0;
         nonempty_s = 0;
+        sorted_s = 0;
         loss_s = 0.f;
     }
     __syncthreads();
@@ -568,20 +584,23 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     hist[tid] = 0;
     __syncthreads();
 
-    // the sample through the model: its bucket histogram
-    for (uint32_t i = tid; i < m; i += blockDim.x) atomicAdd(&hist[learned_bucket<K>(L, smp[i])], 1u);
-    __syncthreads();
-    const uint32_t c = hist[tid];
-    if (c) {
-        atomicMax(&max_s, c);
-        atomicAdd(&nonempty_s, 1u);
-    }
     // the "equal" bucket of each heavy model bucket r is base_id[r] + 1
     if (tid < NB / 32) L.bucket_eq[tid] = 0;
     __syncthreads();
     if ((uint32_t)tid < nmodel && L.heavy_flag[tid]) {
         const uint32_t e = (uint32_t)L.base_id[tid] + 1;
         atomicOr(&L.bucket_eq[e >> 5], 1u << (e & 31));
+    }
+    // the sample through the model: its bucket histogram, and the balance of
+    // the buckets that are sorted further (an equal bucket holds one key
+    // value, however many times it repeats, and is only copied)
+    for (uint32_t i = tid; i < m; i += blockDim.x) atomicAdd(&hist[learned_bucket<K>(L, smp[i])], 1u);
+    __syncthreads();
+    const uint32_t c = hist[tid];
+    if (c && !((L.bucket_eq[tid >> 5] >> (tid & 31)) & 1u)) {
+        atomicMax(&max_s, c);
+        atomicAdd(&nonempty_s, 1u);
+        atomicAdd(&sorted_s, c);
     }
     const double scale = (double)sd.count / (double)m;
     uint64_t cap = 0;
@@ -604,7 +623,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     atomicAdd(&loss_s, lfs / (float)m);
     __syncthreads();
     if (tid == 0) {
-        const float mean = nonempty_s ? (float)m / (float)nonempty_s : 1.f;
+        const float mean = nonempty_s ? (float)sorted_s / (float)nonempty_s : 1.f;
         L.max_over_mean = (float)max_s / mean;
         L.balanced = (L.max_over_mean <= max_imbalance && L.nbuckets <= (uint32_t)NB) ? 1u : 0u;
         L.ok = (L.balanced && L.searches) ? 1u : 0u;

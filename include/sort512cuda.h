@@ -226,16 +226,16 @@ S512_API int s512_segsort_plan_destroy(s512_segsort_plan* plan);
  *     (int32 ^ 0x80000000) or uint64 (IEEE total-order bits of a double, or
  *     (key,value) packed), ascending, in device memory.
  *     s512_learned_root_grad: loss and dL/dtheta of the root piecewise-linear
- *     CDF (64 pieces, slopes theta^2) for the given theta (host, 64 floats).
+ *     CDF (256 pieces, slopes theta^2) for the given theta (host, 256 floats).
  *     s512_learned_fit: fit the whole model to a sorted sample of a segment of
  *     seg_count keys, as a partition level does (m must be the sample size the
  *     library draws for that segment); optional per-bucket sample histogram. */
-#define S512_LEARNED_ROOT_PIECES 64
+#define S512_LEARNED_ROOT_PIECES 256
 typedef struct s512_learned_report {
     float loss_init;      /* root loss at its histogram initialisation */
     float loss_root;      /* root loss after training */
     float loss_final;     /* loss of root + leaves */
-    float max_over_mean;  /* largest bucket / mean bucket, sample counts */
+    float max_over_mean;  /* largest bucket / mean bucket, sample counts (equal buckets aside) */
     uint32_t nbuckets, nmodel;
     uint32_t ok;          /* the model would route the segment: balanced, and the plain splitter table
                              would search for many keys (clustered keys) */

@@ -1,7 +1,7 @@
 """CPU oracle of the learned splitter model's root -- TEST INFRASTRUCTURE ONLY.
 
 The model is this project's own (the reference has no learned part): a
-piecewise-linear CDF of 64 pieces over z = (key - kmin) / (kmax - kmin) with
+piecewise-linear CDF of 256 pieces over z = (key - kmin) / (kmax - kmin) with
 slopes w = theta^2.  This module recomputes, in float64, the loss the device
 trainer minimises and its analytic gradient, so the device's hand-written
 forward/backward pass can be checked against it; finite differences check the
@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import numpy as np
 
-R = 64
+R = 256
 
 
 def encode_i32(x: np.ndarray) -> np.ndarray:
