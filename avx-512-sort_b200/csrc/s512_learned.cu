@@ -11,9 +11,9 @@ __global__ void __launch_bounds__(LR_THREADS) root_grad_kernel(const K* __restri
                                                                const float* __restrict__ theta, float* __restrict__ out) {
     __shared__ double mom[LR_ROOT][RM_COUNT];
     __shared__ uint32_t pstart[LR_ROOT + 1];
-    const K kmin = smp[0], range = smp[m - 1] - smp[0];
-    const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
-    root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
+    RootMap<K> rm;
+    rm.init(smp[0], smp[m - 1]);
+    root_moments<K>(smp, m, rm, pstart, mom);
     if (threadIdx.x < 32) {
         const int l = threadIdx.x;
         float th[RP];

@@ -4,12 +4,16 @@
 // slot table and compares.  The plain splitters stay as the fallback.
 //
 // Model (all slopes non-negative, so the map is monotone by construction):
-//   z   = float(key - kmin) * inv_range                      (saturating at 0)
-//   p0  = c[s] + w[s] * (z*R - s),   s = clamp(floor(z*R))   (root: R pieces)
-//   l   = clamp(floor(p0 * LEAVES))                           (leaf choice)
-//   p   = clamp(a[l] + b[l] * float(key - base[l]), lo[l], hi[l])
-//   r   = min(floor(p * nmodel), nmodel - 1)                  (model bucket)
-// with w = theta^2 >= 0 (root slopes), c the running sum of w, b >= 0, and
+//   zr  = float(min((key - kmin) >> rsh, rspan)) * R / rspan   (saturating at 0)
+//   p0  = c[s] + w[s] * min(zr - s, 1),   s = cell(zr, R)        (root: R pieces)
+//   l   = cell(p0 * LEAVES, LEAVES)                               (leaf choice)
+//   p   = clamp(a[l] + b[l] * float(min((key - base[l]) >> sh[l], span[l])), lo[l], hi[l])
+//   r   = cell(p * nmodel, nmodel)                                (model bucket)
+// where shifts cut key offsets to 23 bits (their floats are then exact) and
+// cell(x, n) is the nearest integer of x - 1/2 clamped to [0, n-1] (floor(x)
+// but at odd integers), both computed without conversion instructions.
+// with w = theta^2 >= 0 (root slopes; each trimmed so that c[s] + w[s] <=
+// c[s+1] in float arithmetic), c the running sum of w, b >= 0, and
 // [lo[l], hi[l]] the sample-CDF range of leaf l, so that every leaf's outputs
 // lie above the previous leaf's.  Each step is a non-decreasing function of
 // the previous one, in IEEE arithmetic too, hence keys map to buckets in key
@@ -59,10 +63,15 @@ constexpr int LR_LEAF_ITERS = 8;
 constexpr float LR_STEP = 0.02f;  // Adam step, relative to the parameters' scale
 constexpr float LR_TABLE_SEARCH_FRAC = 0.25f;
 
+// A leaf: p = a + b * u with u the float of min((key - base) >> sh, span),
+// clamped to the leaf's sample-CDF range [lo, hi].
 template <typename K>
 struct LeafParam {
-    K base;
-    float a, b, lo, hi;
+    K base;          // the leaf's first sample key
+    float a, b;
+    float lo, hi;
+    uint32_t sh;     // (key - base) >> sh has at most 23 bits over the leaf's samples
+    uint32_t span;   // (last sample key - base) >> sh, < 2^23
 };
 
 template <typename K>
@@ -70,14 +79,14 @@ struct LearnedSet {
     // the model: everything inference reads, first, so that the partition
     // pass can copy just this prefix (up to region_off) into shared memory
     K kmin;
-    float inv_range;
+    uint32_t rsh;        // (key - kmin) >> rsh has at most 23 bits over the sample
+    uint32_t rspan;      // (kmax - kmin) >> rsh
+    float zscale;        // LR_ROOT / rspan
     uint32_t nmodel;     // model buckets
-    float rc[LR_ROOT];   // root: value at the start of each piece (normalised)
-    float rw[LR_ROOT];   // root: slope of each piece (normalised, >= 0)
+    float2 rcw[LR_ROOT]; // root piece: (value at its start, slope), normalised, monotone across pieces
     LeafParam<K> leaf[LR_LEAVES];
-    K heavy[NB];         // per model bucket: its heavy key (if heavy_flag)
-    uint8_t heavy_flag[NB];
-    uint8_t base_id[NB]; // first bucket id of each model bucket
+    K heavy[NB];         // per model bucket: its heavy key (if flagged)
+    uint16_t bid[NB];    // per model bucket: first bucket id | 0x100 if it has a heavy key
     // bucket layout and diagnostics
     uint64_t region_off[NB];
     uint64_t region_cap[NB];
@@ -92,58 +101,109 @@ struct LearnedSet {
 };
 
 // ---------------------------------------------------------------------------
-// inference
+// inference (no integer <-> float conversion instructions: offsets are cut to
+// 23 bits and placed in a float's mantissa, indices are rounded by adding
+// 1.5 * 2^23; every step is non-decreasing in its input)
 
-__device__ __forceinline__ float key_to_float(uint32_t d) { return __uint2float_rn(d); }
-__device__ __forceinline__ float key_to_float(uint64_t d) { return __ull2float_rn(d); }
+// The exact float of v < 2^23.
+__device__ __forceinline__ float u23_to_float(uint32_t v) { return __uint_as_float(0x4B000000u | v) - 8388608.0f; }
 
-// The root piece of a key (pieces split [kmin, kmin + range] evenly) and its
-// place inside the piece, in [0, 1].
+// Index cell of x in [0, n] for n <= 2^21: the nearest integer of x - 1/2
+// (ties to even), clamped to [0, n - 1], as int and as float.  Non-decreasing
+// in x; equal to floor(x) except at odd integers x, which fall in cell x - 1.
+__device__ __forceinline__ int cell_of(float x, int n, float* cf) {
+    const float t = (x - 0.5f) + 12582912.0f;
+    int i = __float_as_int(t) - 0x4B400000;
+    float f = t - 12582912.0f;
+    i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
+    f = fminf(fmaxf(f, 0.f), (float)(n - 1));
+    *cf = f;
+    return i;
+}
+
+// min((key - base) >> sh, span) for key >= base (0 below base): the 23-bit
+// offset a leaf or the root turns into a float.
 template <typename K>
-__device__ __forceinline__ int root_piece(K kmin, float inv_range, K key, float* frac) {
-    const K d = key > kmin ? key - kmin : K(0);
-    const float zr = key_to_float(d) * inv_range * (float)LR_ROOT;
-    int s = (int)zr;
-    s = s < 0 ? 0 : (s > LR_ROOT - 1 ? LR_ROOT - 1 : s);
-    *frac = zr - (float)s;
-    return s;
+__device__ __forceinline__ uint32_t key_off23(K key, K base, uint32_t sh, uint32_t span) {
+    const K d = key > base ? key - base : K(0);
+    const K q = d >> sh;
+    return q < (K)span ? (uint32_t)q : span;
+}
+
+// Shift that brings a key range to at most 23 bits.
+template <typename K>
+__device__ __forceinline__ uint32_t shift23(K range) {
+    int nb;
+    if constexpr (sizeof(K) == 8) nb = 64 - __clzll((long long)range);
+    else nb = 32 - __clz((int)range);
+    return nb > 23 ? (uint32_t)(nb - 23) : 0u;
+}
+
+// The root's key map: pieces split [kmin, kmin + range] evenly.
+template <typename K>
+struct RootMap {
+    K kmin;
+    uint32_t rsh, rspan;
+    float zscale;
+    __device__ __forceinline__ void init(K lo, K hi) {
+        kmin = lo;
+        rsh = shift23<K>(hi - lo);
+        rspan = (uint32_t)((hi - lo) >> rsh);
+        zscale = rspan ? (float)LR_ROOT / u23_to_float(rspan) : 0.f;
+    }
+    // piece of a key and its place inside the piece, in [0, 1]
+    __device__ __forceinline__ int piece(K key, float* frac) const {
+        const float zr = u23_to_float(key_off23<K>(key, kmin, rsh, rspan)) * zscale;
+        float sf;
+        const int s = cell_of(zr, LR_ROOT, &sf);
+        *frac = fminf(zr - sf, 1.f);
+        return s;
+    }
+};
+
+template <typename K>
+__device__ __forceinline__ RootMap<K> root_map_of(const LearnedSet<K>& L) {
+    RootMap<K> r;
+    r.kmin = L.kmin;
+    r.rsh = L.rsh;
+    r.rspan = L.rspan;
+    r.zscale = L.zscale;
+    return r;
 }
 
 template <typename K>
-__device__ __forceinline__ float root_p0(const float* rc, const float* rw, K kmin, float inv_range, K key) {
+__device__ __forceinline__ float root_p0(const LearnedSet<K>& L, K key) {
     float frac;
-    const int s = root_piece<K>(kmin, inv_range, key, &frac);
-    return rc[s] + rw[s] * frac;
+    const int s = root_map_of<K>(L).piece(key, &frac);
+    const float2 cw = L.rcw[s];
+    return cw.x + cw.y * frac;
 }
 
-template <typename K>
 __device__ __forceinline__ int leaf_of(float p0) {
-    int l = (int)(p0 * (float)LR_LEAVES);
-    return l < 0 ? 0 : (l > LR_LEAVES - 1 ? LR_LEAVES - 1 : l);
+    float lf;
+    return cell_of(p0 * (float)LR_LEAVES, LR_LEAVES, &lf);
 }
 
 template <typename K>
 __device__ __forceinline__ float leaf_p(const LeafParam<K>& lp, K key) {
-    const K du = key > lp.base ? key - lp.base : K(0);
-    const float p = lp.a + lp.b * key_to_float(du);
-    return fminf(fmaxf(p, lp.lo), lp.hi);
+    const float u = u23_to_float(key_off23<K>(key, lp.base, lp.sh, lp.span));
+    return fminf(fmaxf(lp.a + lp.b * u, lp.lo), lp.hi);
 }
 
-template <typename K>
 __device__ __forceinline__ uint32_t model_bucket(float p, uint32_t nmodel) {
-    int r = (int)(p * (float)nmodel);
-    r = r < 0 ? 0 : r;
-    return (uint32_t)r > nmodel - 1 ? nmodel - 1 : (uint32_t)r;
+    float rf;
+    return (uint32_t)cell_of(p * (float)nmodel, (int)nmodel, &rf);
 }
 
 // bucket id of a key under a learned set held in shared memory
 template <typename K>
 __device__ __forceinline__ uint32_t learned_bucket(const LearnedSet<K>& L, K key) {
-    const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, key);
-    const LeafParam<K>& lp = L.leaf[leaf_of<K>(p0)];
-    const uint32_t r = model_bucket<K>(leaf_p<K>(lp, key), L.nmodel);
-    uint32_t id = L.base_id[r];
-    if (L.heavy_flag[r]) {
+    const float p0 = root_p0<K>(L, key);
+    const LeafParam<K>& lp = L.leaf[leaf_of(p0)];
+    const uint32_t r = model_bucket(leaf_p<K>(lp, key), L.nmodel);
+    const uint32_t e = L.bid[r];
+    uint32_t id = e & 0xFFu;
+    if (e >> 8) {
         const K h = L.heavy[r];
         id += key < h ? 0u : (key == h ? 1u : 2u);
     }
@@ -153,14 +213,23 @@ __device__ __forceinline__ uint32_t learned_bucket(const LearnedSet<K>& L, K key
 // ---------------------------------------------------------------------------
 // training
 
+// Adam with b1 = 0.9, b2 = 0.999.  The bias corrections depend on the step
+// only, so the caller keeps them (AdamBias) for all its parameters.
+constexpr float ADAM_B1 = 0.9f, ADAM_B2 = 0.999f;
+struct AdamBias {
+    float p1 = 1.f, p2 = 1.f;  // b1^t, b2^t
+    __device__ __forceinline__ void next() {
+        p1 *= ADAM_B1;
+        p2 *= ADAM_B2;
+    }
+};
 struct Adam {
     float m = 0.f, v = 0.f;
-    __device__ __forceinline__ float step(float g, float lr, int t) {
-        const float b1 = 0.9f, b2 = 0.999f;
-        m = b1 * m + (1.f - b1) * g;
-        v = b2 * v + (1.f - b2) * g * g;
-        const float mh = m / (1.f - powf(b1, (float)t));
-        const float vh = v / (1.f - powf(b2, (float)t));
+    __device__ __forceinline__ float step(float g, float lr, const AdamBias& bc) {
+        m = ADAM_B1 * m + (1.f - ADAM_B1) * g;
+        v = ADAM_B2 * v + (1.f - ADAM_B2) * g * g;
+        const float mh = m / (1.f - bc.p1);
+        const float vh = v / (1.f - bc.p2);
         return lr * mh / (sqrtf(vh) + 1e-8f);
     }
 };
@@ -180,15 +249,15 @@ constexpr int RM_N = 0, RM_F = 1, RM_FF = 2, RM_Y = 3, RM_YY = 4, RM_YF = 5, RM_
 // Block-wide.  pstart[t] (LR_ROOT + 1 entries) receives the first sample of
 // piece t (samples are sorted and the piece is monotone in the key).
 template <typename K>
-__device__ void root_moments(const K* smp, uint32_t m, K kmin, float inv_range, uint32_t* pstart,
+__device__ void root_moments(const K* smp, uint32_t m, const RootMap<K>& rm, uint32_t* pstart,
                              double (*mom)[RM_COUNT]) {
     const int tid = threadIdx.x;
     for (int t = tid; t <= LR_ROOT; t += blockDim.x) pstart[t] = m;
     __syncthreads();
     for (uint32_t i = tid; i < m; i += blockDim.x) {
         float f;
-        const int s = root_piece<K>(kmin, inv_range, smp[i], &f);
-        const int sp = i == 0 ? -1 : root_piece<K>(kmin, inv_range, smp[i - 1], &f);
+        const int s = rm.piece(smp[i], &f);
+        const int sp = i == 0 ? -1 : rm.piece(smp[i - 1], &f);
         for (int q = sp + 1; q <= s; ++q) pstart[q] = i;
     }
     __syncthreads();
@@ -198,7 +267,7 @@ __device__ void root_moments(const K* smp, uint32_t m, K kmin, float inv_range, 
         double a[RM_COUNT] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         for (uint32_t i = pstart[t] + lane; i < pstart[t + 1]; i += 32) {
             float ff;
-            (void)root_piece<K>(kmin, inv_range, smp[i], &ff);
+            (void)rm.piece(smp[i], &ff);
             const double f = (double)ff, y = ((double)i + 0.5) * inv_m;
             a[RM_N] += 1.0;
             a[RM_F] += f;
@@ -325,14 +394,14 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
         return;
     }
     const K kmin = smp[0], kmax = smp[m - 1];
-    const K range = kmax - kmin;
-    const float inv_range = range ? 1.0f / key_to_float(range) : 0.f;
+    RootMap<K> rm;
+    rm.init(kmin, kmax);
 
     // the training data (per-piece sums), then Adam on theta in warp 0, two
     // pieces a lane, from the histogram start theta = sqrt(n_t / m); the
     // parameters with the lowest loss seen are kept, so training never ends
     // worse than its start
-    root_moments<K>(smp, m, kmin, inv_range, pstart, mom);
+    root_moments<K>(smp, m, rm, pstart, mom);
     static_assert(LR_ROOT % 32 == 0, "whole pieces per lane of warp 0");
     if (tid < 32) {
         float th[RP], best_th[RP];
@@ -340,6 +409,7 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
 #pragma unroll
         for (int k = 0; k < RP; ++k) best_th[k] = th[k] = sqrtf((float)(mom[tid * RP + k][RM_N] / (double)m));
         double best = 1e300, first = 0.0;
+        AdamBias bc;
         for (int it = 0; it <= LR_ITERS; ++it) {
             double loss, g[RP];
             root_eval_warp(mom, m, th, &loss, g);
@@ -350,8 +420,9 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
                 for (int k = 0; k < RP; ++k) best_th[k] = th[k];
             }
             if (it == LR_ITERS) break;
+            bc.next();
 #pragma unroll
-            for (int k = 0; k < RP; ++k) th[k] -= opt[k].step((float)(g[k] * 2.0 * th[k]), LR_STEP * 0.125f, it + 1);
+            for (int k = 0; k < RP; ++k) th[k] -= opt[k].step((float)(g[k] * 2.0 * th[k]), LR_STEP * 0.125f, bc);
         }
 #pragma unroll
         for (int k = 0; k < RP; ++k) rw[tid * RP + k] = best_th[k] * best_th[k];
@@ -361,19 +432,28 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
         }
     }
     __syncthreads();
-    // the kept root, normalised so that it spans [0, 1]
+    // the kept root, normalised so that it spans [0, 1].  Piece t starts at
+    // c_t (rounded from the exact running sum) and its slope is the largest
+    // float w with c_t + w <= c_{t+1} in float arithmetic, so p0 never
+    // decreases from the end of one piece to the start of the next
     if (tid == 0) {
-        float tot = 0.f;
-        for (int t = 0; t < LR_ROOT; ++t) tot += rw[t];
-        const float inv = tot > 0.f ? 1.f / tot : 0.f;
-        float c = 0.f;
+        double tot = 0.0;
+        for (int t = 0; t < LR_ROOT; ++t) tot += (double)rw[t];
+        const double inv = tot > 0.0 ? 1.0 / tot : 0.0;
+        double c = 0.0;
+        float start = 0.f;
         for (int t = 0; t < LR_ROOT; ++t) {
-            L.rc[t] = c * inv;
-            L.rw[t] = rw[t] * inv;
-            c += rw[t];
+            c += (double)rw[t];
+            const float next = t == LR_ROOT - 1 ? 1.f : (float)(c * inv);
+            float w = fmaxf(__fsub_rn(next, start), 0.f);
+            while (w > 0.f && __fadd_rn(start, w) > next) w = nextafterf(w, 0.f);
+            L.rcw[t] = make_float2(start, w);
+            start = next;
         }
-        L.kmin = kmin;
-        L.inv_range = inv_range;
+        L.kmin = rm.kmin;
+        L.rsh = rm.rsh;
+        L.rspan = rm.rspan;
+        L.zscale = rm.zscale;
         L.loss_init = loss_init_s;
         L.loss_root = loss_best_s;
         L.fitted = 1;
@@ -384,8 +464,8 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
     for (int l = tid; l <= LR_LEAVES; l += blockDim.x) lf[l] = m;
     __syncthreads();
     for (uint32_t i = tid; i < m; i += blockDim.x) {
-        const int l = leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i]));
-        const int lp = i == 0 ? -1 : leaf_of<K>(root_p0<K>(L.rc, L.rw, kmin, inv_range, smp[i - 1]));
+        const int l = leaf_of(root_p0<K>(L, smp[i]));
+        const int lp = i == 0 ? -1 : leaf_of(root_p0<K>(L, smp[i - 1]));
         for (int q = lp + 1; q <= l; ++q) lf[q] = i;  // leaves lp+1..l start at i
     }
 }
@@ -419,13 +499,14 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
     LeafParam<K> P;
     if (f < e && f < m) {
         const K base = smp[f];
-        const K span = smp[e - 1] - base;
-        const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
-        // least squares on (u, y), u in [0, 1]
+        const uint32_t sh = shift23<K>(smp[e - 1] - base);
+        const uint32_t span = (uint32_t)((smp[e - 1] - base) >> sh);
+        const float inv_span = span ? 1.0f / u23_to_float(span) : 0.f;
+        // least squares on (u, y), u in [0, 1] (u: the 23-bit offset, scaled)
         float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
         const float cnt = (float)(e - f);
         for (uint32_t i = f + lane; i < e; i += 32) {
-            const float u = key_to_float(smp[i] - base) * inv_span;
+            const float u = u23_to_float(key_off23<K>(smp[i], base, sh, span)) * inv_span;
             const float y = ((float)i + 0.5f) / (float)m;
             su += u;
             sy += y;
@@ -448,10 +529,11 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
             // error (forward + backward per step); keep the best pair seen
             float best_a = a, best_beta = beta, best_l = 3.4e38f;
             Adam oa, ob;
+            AdamBias bc;
             for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
                 float ga = 0.f, gb = 0.f, l2 = 0.f;
                 for (uint32_t i = f + lane; i < e; i += 32) {
-                    const float u = key_to_float(smp[i] - base) * inv_span;
+                    const float u = u23_to_float(key_off23<K>(smp[i], base, sh, span)) * inv_span;
                     const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
                     l2 += r * r;
                     ga += r;
@@ -468,21 +550,26 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
                 if (it > LR_LEAF_ITERS) break;
                 ga *= 2.f / cnt;
                 gb *= 2.f / cnt * 2.f * beta;
-                a -= oa.step(ga, LR_STEP / (float)m, it);
-                beta -= ob.step(gb, LR_STEP / (float)m, it);
+                bc.next();
+                a -= oa.step(ga, LR_STEP / (float)m, bc);
+                beta -= ob.step(gb, LR_STEP / (float)m, bc);
             }
             a = best_a;
             beta = best_beta;
         }
         P.base = base;
         P.a = a;
-        P.b = beta * beta * inv_span;  // slope per unit of (key - base)
+        P.b = beta * beta * inv_span;  // slope per unit of the 23-bit offset
         P.lo = ((float)f + 0.5f) / (float)m;
         P.hi = ((float)(e - 1) + 0.5f) / (float)m;
+        P.sh = sh;
+        P.span = span;
     } else {
         P.base = KeyMax<K>::value;
         P.a = 0.f;
         P.b = 0.f;
+        P.sh = 0;
+        P.span = 0;
         P.lo = P.hi = -1.f;  // patched in launch 3: an empty leaf repeats its left neighbour's top
     }
     if (lane == 0) out[sgi].leaf[l] = P;
@@ -498,7 +585,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
                                                             const SegDesc* __restrict__ segs, uint32_t nsegs,
                                                             const SplitSet<K>* __restrict__ plain,
                                                             LearnedSet<K>* __restrict__ out, int key_bytes,
-                                                            float max_imbalance) {
+                                                            float max_imbalance, int report_loss) {
     const uint32_t sgi = blockIdx.x;
     if (sgi >= nsegs) return;
     if (!out[sgi].fitted) return;
@@ -561,22 +648,19 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     if (nmodel < 2) nmodel = 2;
     if (heavy) {
         const K h = ps.uniq[tid];
-        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, h);
-        const uint32_t r = model_bucket<K>(leaf_p<K>(L.leaf[leaf_of<K>(p0)], h), nmodel);
+        const float p0 = root_p0<K>(L, h);
+        const uint32_t r = model_bucket(leaf_p<K>(L.leaf[leaf_of(p0)], h), nmodel);
         atomicMin(&first_heavy[r], (uint32_t)tid);
     }
     __syncthreads();
-    L.heavy_flag[tid] = 0;
-    L.heavy[tid] = K(0);
-    if (first_heavy[tid] != 0xFFFFFFFFu && (uint32_t)tid < nmodel) {
-        L.heavy_flag[tid] = 1;
-        L.heavy[tid] = ps.uniq[first_heavy[tid]];
-    }
+    const bool has_heavy = first_heavy[tid] != 0xFFFFFFFFu && (uint32_t)tid < nmodel;
+    L.heavy[tid] = has_heavy ? ps.uniq[first_heavy[tid]] : K(0);
     // bucket ids: a model bucket is one id, or three (below / equal / above)
     // with a heavy key
-    const uint32_t width = (uint32_t)tid < nmodel ? (L.heavy_flag[tid] ? 3u : 1u) : 0u;
+    const uint32_t width = (uint32_t)tid < nmodel ? (has_heavy ? 3u : 1u) : 0u;
     const uint32_t id = block_exclusive_scan_first<NB, uint32_t>(width, wt32, &tot_ids_s);
-    L.base_id[tid] = (uint8_t)(id < NB ? id : NB - 1);
+    const uint32_t base_id = id < NB ? id : NB - 1;
+    L.bid[tid] = (uint16_t)(base_id | (has_heavy ? 0x100u : 0u));
     if (tid == 0) {
         L.nmodel = nmodel;
         L.nbuckets = tot_ids_s;  // (the scan's total, written by one thread to shared memory)
@@ -587,8 +671,8 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     // the "equal" bucket of each heavy model bucket r is base_id[r] + 1
     if (tid < NB / 32) L.bucket_eq[tid] = 0;
     __syncthreads();
-    if ((uint32_t)tid < nmodel && L.heavy_flag[tid]) {
-        const uint32_t e = (uint32_t)L.base_id[tid] + 1;
+    if (has_heavy) {
+        const uint32_t e = base_id + 1;
         atomicOr(&L.bucket_eq[e >> 5], 1u << (e & 31));
     }
     // the sample through the model: its bucket histogram, and the balance of
@@ -613,14 +697,19 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     const uint64_t off = block_exclusive_scan_first<NB, uint64_t>(cap, wt64, (uint64_t*)nullptr);
     L.region_off[tid] = off;
     L.region_cap[tid] = cap;
-    // final loss of the whole model on the sample (root + leaves)
-    float lfs = 0.f;
-    for (uint32_t i = tid; i < m; i += blockDim.x) {
-        const float p0 = root_p0<K>(L.rc, L.rw, L.kmin, L.inv_range, smp[i]);
-        const float r = leaf_p<K>(L.leaf[leaf_of<K>(p0)], smp[i]) - ((float)i + 0.5f) / (float)m;
-        lfs += r * r;
+    // final loss of the whole model on the sample (root + leaves), for the
+    // fit's report only
+    if (report_loss) {
+        float lfs = 0.f;
+        for (uint32_t i = tid; i < m; i += blockDim.x) {
+            const float p0 = root_p0<K>(L, smp[i]);
+            const float r = leaf_p<K>(L.leaf[leaf_of(p0)], smp[i]) - ((float)i + 0.5f) / (float)m;
+            lfs += r * r;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) lfs += __shfl_xor_sync(0xFFFFFFFFu, lfs, d);
+        if (lane == 0) atomicAdd(&loss_s, lfs / (float)m);
     }
-    atomicAdd(&loss_s, lfs / (float)m);
     __syncthreads();
     if (tid == 0) {
         const float mean = nonempty_s ? (float)sorted_s / (float)nonempty_s : 1.f;
@@ -637,7 +726,8 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
 
 // The three launches of a fit (lfirst: nsegs * (LR_LEAVES + 1) words).
 // force: train every large segment, also where the table would not search
-// (the model is then reported but does not route).
+// (the model is then reported but does not route), and compute the final
+// loss for the report.
 template <typename K>
 static void launch_learned_fit(const K* samples, const SegDesc* segs, uint32_t nsegs, const SplitSet<K>* plain,
                                LearnedSet<K>* out, uint32_t* lfirst, int key_bytes, float max_imbalance,
@@ -645,7 +735,8 @@ static void launch_learned_fit(const K* samples, const SegDesc* segs, uint32_t n
     learned_root_kernel<K><<<nsegs, LR_THREADS, 0, st>>>(samples, segs, nsegs, plain, out, lfirst, key_bytes,
                                                          force);
     learned_leaf_kernel<K><<<(nsegs * LR_LEAVES + 7) / 8, 256, 0, st>>>(samples, segs, nsegs, out, lfirst, key_bytes);
-    learned_finish_kernel<K><<<nsegs, NB, 0, st>>>(samples, segs, nsegs, plain, out, key_bytes, max_imbalance);
+    learned_finish_kernel<K><<<nsegs, NB, 0, st>>>(samples, segs, nsegs, plain, out, key_bytes, max_imbalance,
+                                                   force);
 }
 
 }  // namespace s512

@@ -1,8 +1,8 @@
 """CPU oracle of the learned splitter model's root -- TEST INFRASTRUCTURE ONLY.
 
 The model is this project's own (the reference has no learned part): a
-piecewise-linear CDF of 256 pieces over z = (key - kmin) / (kmax - kmin) with
-slopes w = theta^2.  This module recomputes, in float64, the loss the device
+piecewise-linear CDF of 256 pieces over the key range with slopes w = theta^2
+(pieces as root_pieces computes them).  This module recomputes, in float64, the loss the device
 trainer minimises and its analytic gradient, so the device's hand-written
 forward/backward pass can be checked against it; finite differences check the
 analytic gradient itself.
@@ -25,14 +25,22 @@ def encode_f64(x: np.ndarray) -> np.ndarray:
 
 
 def root_pieces(keys: np.ndarray):
-    """Piece index and fraction of every (sorted, encoded) sample key."""
+    """Piece index and fraction of every (sorted, encoded) sample key, in the
+    device's float32 arithmetic: the offset from the smallest key is cut to
+    23 bits (shifted right by bit_length(range) - 23), scaled by
+    R / (range >> shift), and the piece is the nearest integer of zr - 1/2
+    (ties to even) clamped to [0, R-1]; the fraction is min(zr - piece, 1)."""
     k = keys.astype(np.uint64)
-    kmin, kmax = k[0], k[-1]
-    rng = float(kmax - kmin)
-    z = (k - kmin).astype(np.float64) / rng if rng > 0 else np.zeros(len(k))
-    zr = z * R
-    s = np.clip(np.floor(zr), 0, R - 1).astype(np.int64)
-    return s, zr - s
+    kmin = int(k[0])
+    rng = int(k[-1]) - kmin
+    sh = max(rng.bit_length() - 23, 0)
+    rspan = rng >> sh
+    d = np.minimum((k - np.uint64(kmin)) >> np.uint64(sh), np.uint64(rspan)).astype(np.float32)
+    zscale = np.float32(R) / np.float32(rspan) if rspan else np.float32(0.0)
+    zr = (d * zscale).astype(np.float32)
+    sf = np.clip(np.rint(zr - np.float32(0.5)), 0, R - 1).astype(np.float32)
+    frac = np.minimum(zr - sf, np.float32(1.0))
+    return sf.astype(np.int64), frac.astype(np.float64)
 
 
 def root_loss_grad(keys: np.ndarray, theta: np.ndarray):
