@@ -4,14 +4,11 @@
 // slot table and compares.  The plain splitters stay as the fallback.
 //
 // Model (all slopes non-negative, so the map is monotone by construction):
-//   zr  = float(min((key - kmin) >> rsh, rspan)) * R / rspan   (saturating at 0)
-//   p0  = c[s] + w[s] * min(zr - s, 1),   s = cell(zr, R)        (root: R pieces)
-//   l   = cell(p0 * LEAVES, LEAVES)                               (leaf choice)
-//   p   = clamp(a[l] + b[l] * float(min((key - base[l]) >> sh[l], span[l])), lo[l], hi[l])
-//   r   = cell(p * nmodel, nmodel)                                (model bucket)
-// where shifts cut key offsets to 23 bits (their floats are then exact) and
-// cell(x, n) is the nearest integer of x - 1/2 clamped to [0, n-1] (floor(x)
-// but at odd integers), both computed without conversion instructions.
+//   zr  = float(key - kmin) * R / float(kmax - kmin)       (saturating at 0)
+//   p0  = c[s] + w[s] * min(zr - s, 1),   s = min(floor(zr), R - 1)   (root)
+//   l   = clamp(floor(p0 * LEAVES))                           (leaf choice)
+//   p   = clamp(a[l] + b[l] * float(key - base[l]), lo[l], hi[l])
+//   r   = min(floor(p * nmodel), nmodel - 1)                  (model bucket)
 // with w = theta^2 >= 0 (root slopes; each trimmed so that c[s] + w[s] <=
 // c[s+1] in float arithmetic), c the running sum of w, b >= 0, and
 // [lo[l], hi[l]] the sample-CDF range of leaf l, so that every leaf's outputs
@@ -63,15 +60,13 @@ constexpr int LR_LEAF_ITERS = 8;
 constexpr float LR_STEP = 0.02f;  // Adam step, relative to the parameters' scale
 constexpr float LR_TABLE_SEARCH_FRAC = 0.25f;
 
-// A leaf: p = a + b * u with u the float of min((key - base) >> sh, span),
-// clamped to the leaf's sample-CDF range [lo, hi].
+// A leaf: p = a + b * float(key - base) (0 below base), clamped to the
+// leaf's sample-CDF range [lo, hi].
 template <typename K>
 struct LeafParam {
     K base;          // the leaf's first sample key
     float a, b;
     float lo, hi;
-    uint32_t sh;     // (key - base) >> sh has at most 23 bits over the leaf's samples
-    uint32_t span;   // (last sample key - base) >> sh, < 2^23
 };
 
 template <typename K>
@@ -79,9 +74,7 @@ struct LearnedSet {
     // the model: everything inference reads, first, so that the partition
     // pass can copy just this prefix (up to region_off) into shared memory
     K kmin;
-    uint32_t rsh;        // (key - kmin) >> rsh has at most 23 bits over the sample
-    uint32_t rspan;      // (kmax - kmin) >> rsh
-    float zscale;        // LR_ROOT / rspan
+    float zscale;        // LR_ROOT / float(kmax - kmin)
     uint32_t nmodel;     // model buckets
     float2 rcw[LR_ROOT]; // root piece: (value at its start, slope), normalised, monotone across pieces
     LeafParam<K> leaf[LR_LEAVES];
@@ -101,62 +94,27 @@ struct LearnedSet {
 };
 
 // ---------------------------------------------------------------------------
-// inference (no integer <-> float conversion instructions: offsets are cut to
-// 23 bits and placed in a float's mantissa, indices are rounded by adding
-// 1.5 * 2^23; every step is non-decreasing in its input)
+// inference (every step is non-decreasing in its input, in IEEE arithmetic)
 
-// The exact float of v < 2^23.
-__device__ __forceinline__ float u23_to_float(uint32_t v) { return __uint_as_float(0x4B000000u | v) - 8388608.0f; }
+__device__ __forceinline__ float key_to_float(uint32_t d) { return __uint2float_rn(d); }
+__device__ __forceinline__ float key_to_float(uint64_t d) { return __ull2float_rn(d); }
 
-// Index cell of x in [0, n] for n <= 2^21: the nearest integer of x - 1/2
-// (ties to even), clamped to [0, n - 1], as int and as float.  Non-decreasing
-// in x; equal to floor(x) except at odd integers x, which fall in cell x - 1.
-__device__ __forceinline__ int cell_of(float x, int n, float* cf) {
-    const float t = (x - 0.5f) + 12582912.0f;
-    int i = __float_as_int(t) - 0x4B400000;
-    float f = t - 12582912.0f;
-    i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
-    f = fminf(fmaxf(f, 0.f), (float)(n - 1));
-    *cf = f;
-    return i;
-}
-
-// min((key - base) >> sh, span) for key >= base (0 below base): the 23-bit
-// offset a leaf or the root turns into a float.
-template <typename K>
-__device__ __forceinline__ uint32_t key_off23(K key, K base, uint32_t sh, uint32_t span) {
-    const K d = key > base ? key - base : K(0);
-    const K q = d >> sh;
-    return q < (K)span ? (uint32_t)q : span;
-}
-
-// Shift that brings a key range to at most 23 bits.
-template <typename K>
-__device__ __forceinline__ uint32_t shift23(K range) {
-    int nb;
-    if constexpr (sizeof(K) == 8) nb = 64 - __clzll((long long)range);
-    else nb = 32 - __clz((int)range);
-    return nb > 23 ? (uint32_t)(nb - 23) : 0u;
-}
-
-// The root's key map: pieces split [kmin, kmin + range] evenly.
+// The root's key map: pieces split [kmin, kmax] evenly.
 template <typename K>
 struct RootMap {
     K kmin;
-    uint32_t rsh, rspan;
     float zscale;
     __device__ __forceinline__ void init(K lo, K hi) {
         kmin = lo;
-        rsh = shift23<K>(hi - lo);
-        rspan = (uint32_t)((hi - lo) >> rsh);
-        zscale = rspan ? (float)LR_ROOT / u23_to_float(rspan) : 0.f;
+        zscale = hi > lo ? (float)LR_ROOT / key_to_float(hi - lo) : 0.f;
     }
     // piece of a key and its place inside the piece, in [0, 1]
     __device__ __forceinline__ int piece(K key, float* frac) const {
-        const float zr = u23_to_float(key_off23<K>(key, kmin, rsh, rspan)) * zscale;
-        float sf;
-        const int s = cell_of(zr, LR_ROOT, &sf);
-        *frac = fminf(zr - sf, 1.f);
+        const K d = key > kmin ? key - kmin : K(0);
+        const float zr = key_to_float(d) * zscale;
+        int s = (int)zr;
+        s = s > LR_ROOT - 1 ? LR_ROOT - 1 : s;
+        *frac = fminf(zr - (float)s, 1.f);
         return s;
     }
 };
@@ -165,8 +123,6 @@ template <typename K>
 __device__ __forceinline__ RootMap<K> root_map_of(const LearnedSet<K>& L) {
     RootMap<K> r;
     r.kmin = L.kmin;
-    r.rsh = L.rsh;
-    r.rspan = L.rspan;
     r.zscale = L.zscale;
     return r;
 }
@@ -180,19 +136,20 @@ __device__ __forceinline__ float root_p0(const LearnedSet<K>& L, K key) {
 }
 
 __device__ __forceinline__ int leaf_of(float p0) {
-    float lf;
-    return cell_of(p0 * (float)LR_LEAVES, LR_LEAVES, &lf);
+    const int l = (int)(p0 * (float)LR_LEAVES);
+    return l < 0 ? 0 : (l > LR_LEAVES - 1 ? LR_LEAVES - 1 : l);
 }
 
 template <typename K>
 __device__ __forceinline__ float leaf_p(const LeafParam<K>& lp, K key) {
-    const float u = u23_to_float(key_off23<K>(key, lp.base, lp.sh, lp.span));
-    return fminf(fmaxf(lp.a + lp.b * u, lp.lo), lp.hi);
+    const K du = key > lp.base ? key - lp.base : K(0);
+    return fminf(fmaxf(lp.a + lp.b * key_to_float(du), lp.lo), lp.hi);
 }
 
 __device__ __forceinline__ uint32_t model_bucket(float p, uint32_t nmodel) {
-    float rf;
-    return (uint32_t)cell_of(p * (float)nmodel, (int)nmodel, &rf);
+    int r = (int)(p * (float)nmodel);
+    r = r < 0 ? 0 : r;
+    return (uint32_t)r > nmodel - 1 ? nmodel - 1 : (uint32_t)r;
 }
 
 // bucket id of a key under a learned set held in shared memory
@@ -451,8 +408,6 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
             start = next;
         }
         L.kmin = rm.kmin;
-        L.rsh = rm.rsh;
-        L.rspan = rm.rspan;
         L.zscale = rm.zscale;
         L.loss_init = loss_init_s;
         L.loss_root = loss_best_s;
@@ -499,14 +454,13 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
     LeafParam<K> P;
     if (f < e && f < m) {
         const K base = smp[f];
-        const uint32_t sh = shift23<K>(smp[e - 1] - base);
-        const uint32_t span = (uint32_t)((smp[e - 1] - base) >> sh);
-        const float inv_span = span ? 1.0f / u23_to_float(span) : 0.f;
-        // least squares on (u, y), u in [0, 1] (u: the 23-bit offset, scaled)
+        const K span = smp[e - 1] - base;
+        const float inv_span = span ? 1.0f / key_to_float(span) : 0.f;
+        // least squares on (u, y), u in [0, 1]
         float su = 0.f, sy = 0.f, suu = 0.f, suy = 0.f;
         const float cnt = (float)(e - f);
         for (uint32_t i = f + lane; i < e; i += 32) {
-            const float u = u23_to_float(key_off23<K>(smp[i], base, sh, span)) * inv_span;
+            const float u = key_to_float(smp[i] - base) * inv_span;
             const float y = ((float)i + 0.5f) / (float)m;
             su += u;
             sy += y;
@@ -533,7 +487,7 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
             for (int it = 1; it <= LR_LEAF_ITERS + 1; ++it) {
                 float ga = 0.f, gb = 0.f, l2 = 0.f;
                 for (uint32_t i = f + lane; i < e; i += 32) {
-                    const float u = u23_to_float(key_off23<K>(smp[i], base, sh, span)) * inv_span;
+                    const float u = key_to_float(smp[i] - base) * inv_span;
                     const float r = a + beta * beta * u - ((float)i + 0.5f) / (float)m;
                     l2 += r * r;
                     ga += r;
@@ -559,17 +513,13 @@ __global__ void __launch_bounds__(256) learned_leaf_kernel(const K* __restrict__
         }
         P.base = base;
         P.a = a;
-        P.b = beta * beta * inv_span;  // slope per unit of the 23-bit offset
+        P.b = beta * beta * inv_span;  // slope per unit of (key - base)
         P.lo = ((float)f + 0.5f) / (float)m;
         P.hi = ((float)(e - 1) + 0.5f) / (float)m;
-        P.sh = sh;
-        P.span = span;
     } else {
         P.base = KeyMax<K>::value;
         P.a = 0.f;
         P.b = 0.f;
-        P.sh = 0;
-        P.span = 0;
         P.lo = P.hi = -1.f;  // patched in launch 3: an empty leaf repeats its left neighbour's top
     }
     if (lane == 0) out[sgi].leaf[l] = P;

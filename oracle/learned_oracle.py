@@ -26,21 +26,16 @@ def encode_f64(x: np.ndarray) -> np.ndarray:
 
 def root_pieces(keys: np.ndarray):
     """Piece index and fraction of every (sorted, encoded) sample key, in the
-    device's float32 arithmetic: the offset from the smallest key is cut to
-    23 bits (shifted right by bit_length(range) - 23), scaled by
-    R / (range >> shift), and the piece is the nearest integer of zr - 1/2
-    (ties to even) clamped to [0, R-1]; the fraction is min(zr - piece, 1)."""
+    device's float32 arithmetic: zr = float32(key - kmin) * (R / float32(kmax -
+    kmin)), piece = min(floor(zr), R - 1), fraction = min(zr - piece, 1)."""
     k = keys.astype(np.uint64)
-    kmin = int(k[0])
-    rng = int(k[-1]) - kmin
-    sh = max(rng.bit_length() - 23, 0)
-    rspan = rng >> sh
-    d = np.minimum((k - np.uint64(kmin)) >> np.uint64(sh), np.uint64(rspan)).astype(np.float32)
-    zscale = np.float32(R) / np.float32(rspan) if rspan else np.float32(0.0)
-    zr = (d * zscale).astype(np.float32)
-    sf = np.clip(np.rint(zr - np.float32(0.5)), 0, R - 1).astype(np.float32)
-    frac = np.minimum(zr - sf, np.float32(1.0))
-    return sf.astype(np.int64), frac.astype(np.float64)
+    kmin = k[0]
+    rng = k[-1] - kmin
+    zscale = np.float32(R) / np.float32(rng) if rng > 0 else np.float32(0.0)
+    zr = ((k - kmin).astype(np.float32) * zscale).astype(np.float32)
+    s = np.minimum(np.floor(zr), np.float32(R - 1)).astype(np.float32)
+    frac = np.minimum(zr - s, np.float32(1.0))
+    return s.astype(np.int64), frac.astype(np.float64)
 
 
 def root_loss_grad(keys: np.ndarray, theta: np.ndarray):
