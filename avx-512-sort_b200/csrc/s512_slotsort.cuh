@@ -1,8 +1,9 @@
 // s512_slotsort.cuh -- one bucket sorted by distribution counting: keys are
 // dealt into value slots by a monotone linear map of their offset from the
 // bucket's minimum, the slots are laid out by an exclusive scan of their
-// counts, and every key finds its final place by ranking itself inside its
-// own (short) slot.
+// counts, the keys are dealt into their slots, and each slot that received
+// more than one key (a few keys at most) is put in order in place by the
+// thread that scanned it; the buffer is then the sorted bucket.
 //
 // A bucket that reaches the leaf stage holds the keys between two adjacent
 // quantile splitters, so its values are close to evenly spread over
@@ -16,16 +17,15 @@
 // sorted by the bitonic + merge-path block sort instead (s512_blocksort.cuh).
 //
 // Equal keys are identical encoded words (see s512_common.cuh), so placing
-// ties in any order gives the same output; the in-slot rank breaks ties by
-// shared-memory position only to make the ranks a permutation.
+// ties in any order gives the same output.
 #pragma once
 
 #include "s512_blocksort.cuh"
 
 namespace s512 {
 
-constexpr uint32_t SLOT_MAX_RUN = 32;  // largest slot ranked key by key
-constexpr uint32_t SLOT_SUMSQ = 4;     // ranking work allowed per key
+constexpr uint32_t SLOT_MAX_RUN = 32;  // largest slot put in order by one thread
+constexpr uint32_t SLOT_SUMSQ = 4;     // in-slot ordering work (sum of squared counts) allowed per key
 
 // Monotone map from a key in [lo, hi] to a slot in [0, nslots): the offset
 // x - lo is cut to its 32 leading significant bits (shift sh), then either
@@ -65,14 +65,14 @@ struct SlotRed {
 };
 
 // Shared memory of block_slot_sort for a block of THREADS x IPT keys: the
-// key buffer (padded for the block sort when that runs inline, INLINE), the
-// counters, and one bit per slot that marks slots of more than one key.
+// key buffer (padded for the block sort when that runs inline, INLINE) and
+// the counters.
 template <typename K, int THREADS, int IPT, bool INLINE = true>
 struct SlotSmem {
     static constexpr uint32_t S = (uint32_t)THREADS * IPT;
     static constexpr size_t keys_bytes = ((size_t)(INLINE ? padded_len(S) : S) * sizeof(K) + 15) & ~(size_t)15;
     static constexpr size_t ctr_bytes = (size_t)S * sizeof(uint32_t);
-    static constexpr size_t bytes = keys_bytes + ctr_bytes + (size_t)S / 8;
+    static constexpr size_t bytes = keys_bytes + ctr_bytes;
 };
 
 // Sort the c <= THREADS*IPT keys held striped in key[] (element
@@ -93,11 +93,10 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
                                 unsigned char* smem, SlotRed<K>& red) {
     constexpr uint32_t S = (uint32_t)THREADS * IPT;
     constexpr int NW = THREADS / 32;
-    static_assert(IPT % 4 == 0 && 32 % IPT == 0, "counters are read four at a time, slot bits in whole words");
+    static_assert(IPT % 4 == 0 && IPT <= 32, "counters are read four at a time, slot bits in one word");
     using SM = SlotSmem<K, THREADS, IPT, INLINE_FALLBACK>;
     K* s = reinterpret_cast<K*>(smem);
     uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes);
-    uint32_t* multi = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes + SM::ctr_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
     // 1. bounds of the bucket; counters zeroed
@@ -203,14 +202,6 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
             q = make_uint4(s0, s1, s2, s3);
             *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = q;
         }
-        {
-            // the bits of the 32/IPT threads that share a word of `multi`
-            constexpr int G = 32 / IPT;
-            uint32_t w = G > 1 ? mbits << ((lane % G) * IPT) : mbits;
-#pragma unroll
-            for (int d = 1; d < G; d <<= 1) w |= __shfl_xor_sync(0xFFFFFFFFu, w, d);
-            if (lane % G == 0) multi[(tid * IPT) >> 5] = w;
-        }
         __syncthreads();
         // 4. deal the keys into their slots; afterwards ctr[j] is the end of slot j
 #pragma unroll
@@ -219,24 +210,34 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
         }
         refill();
         __syncthreads();
-        // 5. rank each key inside its slot and write it to its final place;
-        //    the key of a one-key slot is already there (rank p)
-        for (uint32_t p = tid; p < c; p += THREADS) {
-            const K x = s[p];
-            const uint32_t j = f(x);
-            if (!((multi[j >> 5] >> (j & 31)) & 1u)) {
-                store(p, x);
-                continue;
-            }
+        // 5. the keys of a slot of several are in dealing order: the thread
+        //    that scanned the slot puts them in key order, in place
+        for (uint32_t bits = mbits; bits; bits &= bits - 1) {
+            const uint32_t j = tid * IPT + (uint32_t)(__ffs(bits) - 1);
             const uint32_t a = j ? ctr[j - 1] : 0u;
             const uint32_t e = ctr[j];
-            uint32_t rank = a;
-            for (uint32_t q = a; q < e; ++q) {
-                const K y = s[q];
-                rank += (y < x || (y == x && q < p)) ? 1u : 0u;
+            if (e - a == 2) {
+                const K x0 = s[a], x1 = s[a + 1];
+                if (x1 < x0) {
+                    s[a] = x1;
+                    s[a + 1] = x0;
+                }
+            } else {
+                for (uint32_t q = a + 1; q < e; ++q) {
+                    const K x = s[q];
+                    uint32_t k = q;
+                    for (; k > a; --k) {
+                        const K y = s[k - 1];
+                        if (!(x < y)) break;
+                        s[k] = y;
+                    }
+                    s[k] = x;
+                }
             }
-            store(rank, x);
         }
+        __syncthreads();
+        // 6. every key is in its final place
+        for (uint32_t p = tid; p < c; p += THREADS) store(p, s[p]);
     } else if constexpr (INLINE_FALLBACK) {
         // uneven spread: bitonic leaves + merge path on the same keys
 #pragma unroll
