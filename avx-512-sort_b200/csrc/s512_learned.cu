@@ -9,7 +9,7 @@ namespace s512 {
 template <typename K>
 __global__ void __launch_bounds__(LR_THREADS) root_grad_kernel(const K* __restrict__ smp, uint32_t m,
                                                                const float* __restrict__ theta, float* __restrict__ out) {
-    __shared__ double mom[LR_ROOT][RM_COUNT];
+    __shared__ double mom[LR_ROOT * RM_COUNT];
     __shared__ uint32_t pstart[LR_ROOT + 1];
     RootMap<K> rm;
     rm.init(smp[0], smp[m - 1]);

@@ -128,11 +128,16 @@ __device__ __forceinline__ RootMap<K> root_map_of(const LearnedSet<K>& L) {
 }
 
 template <typename K>
-__device__ __forceinline__ float root_p0(const LearnedSet<K>& L, K key) {
+__device__ __forceinline__ float root_p0(const RootMap<K>& rm, const float2* rcw, K key) {
     float frac;
-    const int s = root_map_of<K>(L).piece(key, &frac);
-    const float2 cw = L.rcw[s];
+    const int s = rm.piece(key, &frac);
+    const float2 cw = rcw[s];
     return cw.x + cw.y * frac;
+}
+
+template <typename K>
+__device__ __forceinline__ float root_p0(const LearnedSet<K>& L, K key) {
+    return root_p0<K>(root_map_of<K>(L), L.rcw, key);
 }
 
 __device__ __forceinline__ int leaf_of(float p0) {
@@ -175,9 +180,12 @@ __device__ __forceinline__ uint32_t learned_bucket(const LearnedSet<K>& L, K key
 constexpr float ADAM_B1 = 0.9f, ADAM_B2 = 0.999f;
 struct AdamBias {
     float p1 = 1.f, p2 = 1.f;  // b1^t, b2^t
+    float c1 = 0.f, c2 = 0.f;  // 1 / (1 - b1^t), 1 / (1 - b2^t)
     __device__ __forceinline__ void next() {
         p1 *= ADAM_B1;
         p2 *= ADAM_B2;
+        c1 = 1.f / (1.f - p1);
+        c2 = 1.f / (1.f - p2);
     }
 };
 struct Adam {
@@ -185,9 +193,7 @@ struct Adam {
     __device__ __forceinline__ float step(float g, float lr, const AdamBias& bc) {
         m = ADAM_B1 * m + (1.f - ADAM_B1) * g;
         v = ADAM_B2 * v + (1.f - ADAM_B2) * g * g;
-        const float mh = m / (1.f - bc.p1);
-        const float vh = v / (1.f - bc.p2);
-        return lr * mh / (sqrtf(vh) + 1e-8f);
+        return lr * (m * bc.c1) / (sqrtf(v * bc.c2) + 1e-8f);
     }
 };
 
@@ -202,12 +208,17 @@ struct Adam {
 // difference of these sums); a training step is then O(pieces) work in one
 // warp.
 constexpr int RM_N = 0, RM_F = 1, RM_FF = 2, RM_Y = 3, RM_YY = 4, RM_YF = 5, RM_COUNT = 6;
+// Training runs in one warp, RP = LR_ROOT / 32 consecutive pieces a lane
+// (lane t / RP holds piece t).  The sums of piece t sit at mom[mom_idx(t, c)]:
+// consecutive lanes read consecutive words, free of bank conflicts.
+constexpr int RP = LR_ROOT / 32;
+__host__ __device__ constexpr int mom_idx(int t, int c) { return ((t % RP) * RM_COUNT + c) * 32 + t / RP; }
 
 // Block-wide.  pstart[t] (LR_ROOT + 1 entries) receives the first sample of
 // piece t (samples are sorted and the piece is monotone in the key).
 template <typename K>
 __device__ void root_moments(const K* smp, uint32_t m, const RootMap<K>& rm, uint32_t* pstart,
-                             double (*mom)[RM_COUNT]) {
+                             double* mom) {
     const int tid = threadIdx.x;
     for (int t = tid; t <= LR_ROOT; t += blockDim.x) pstart[t] = m;
     __syncthreads();
@@ -240,7 +251,7 @@ __device__ void root_moments(const K* smp, uint32_t m, const RootMap<K>& rm, uin
         }
         if (lane == 0)
 #pragma unroll
-            for (int k = 0; k < RM_COUNT; ++k) mom[t][k] = a[k];
+            for (int k = 0; k < RM_COUNT; ++k) mom[mom_idx(t, k)] = a[k];
     }
     __syncthreads();
 }
@@ -249,8 +260,7 @@ __device__ void root_moments(const K* smp, uint32_t m, const RootMap<K>& rm, uin
 // loss of the root with w_t = theta_t^2 (rw = w, rc = exclusive running sum
 // of w) and dL/dw_t,
 //   dL/dw_t = (2/m) * (S1_t + sum_{u > t} S0_u).
-constexpr int RP = LR_ROOT / 32;
-__device__ __forceinline__ void root_eval_warp(const double (*mom)[RM_COUNT], uint32_t m, const float (&th)[RP],
+__device__ __forceinline__ void root_eval_warp(const double* mom, uint32_t m, const float (&th)[RP],
                                                double* loss, double (&g)[RP]) {
     const int lane = threadIdx.x & 31;
     double w[RP], lane_w = 0.0;
@@ -269,12 +279,13 @@ __device__ __forceinline__ void root_eval_warp(const double (*mom)[RM_COUNT], ui
     double S0[RP], S1[RP], l = 0.0, lane_s0 = 0.0;
 #pragma unroll
     for (int k = 0; k < RP; ++k) {
-        const double* M = mom[lane * RP + k];
+        const double* M = mom + k * RM_COUNT * 32 + lane;  // M[c * 32]: sum c of piece lane * RP + k
         const double A = rc, B = w[k];
-        S0[k] = M[RM_N] * A + B * M[RM_F] - M[RM_Y];
-        S1[k] = A * M[RM_F] + B * M[RM_FF] - M[RM_YF];
-        l += M[RM_N] * A * A + B * B * M[RM_FF] + M[RM_YY] + 2.0 * A * B * M[RM_F] - 2.0 * A * M[RM_Y] -
-             2.0 * B * M[RM_YF];
+        const double n = M[RM_N * 32], sf = M[RM_F * 32], sff = M[RM_FF * 32];
+        const double sy = M[RM_Y * 32], syy = M[RM_YY * 32], syf = M[RM_YF * 32];
+        S0[k] = n * A + B * sf - sy;
+        S1[k] = A * sf + B * sff - syf;
+        l += n * A * A + B * B * sff + syy + 2.0 * A * B * sf - 2.0 * A * sy - 2.0 * B * syf;
         lane_s0 += S0[k];
         rc += w[k];
     }
@@ -311,10 +322,9 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
                                                                   int force) {
     const uint32_t sgi = blockIdx.x;
     if (sgi >= nsegs) return;
-    __shared__ double mom[LR_ROOT][RM_COUNT];
+    __shared__ double mom[LR_ROOT * RM_COUNT];
     __shared__ uint32_t pstart[LR_ROOT + 1];
-    __shared__ float rw[LR_ROOT];
-    __shared__ float loss_init_s, loss_best_s;
+    __shared__ float2 rcw[LR_ROOT];
     __shared__ uint32_t search_s;
     const SegDesc sd = segs[sgi];
     const int tid = threadIdx.x;
@@ -364,7 +374,7 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
         float th[RP], best_th[RP];
         Adam opt[RP];
 #pragma unroll
-        for (int k = 0; k < RP; ++k) best_th[k] = th[k] = sqrtf((float)(mom[tid * RP + k][RM_N] / (double)m));
+        for (int k = 0; k < RP; ++k) best_th[k] = th[k] = sqrtf((float)(mom[mom_idx(tid * RP + k, RM_N)] / (double)m));
         double best = 1e300, first = 0.0;
         AdamBias bc;
         for (int it = 0; it <= LR_ITERS; ++it) {
@@ -381,46 +391,69 @@ __global__ void __launch_bounds__(LR_THREADS) learned_root_kernel(const K* __res
 #pragma unroll
             for (int k = 0; k < RP; ++k) th[k] -= opt[k].step((float)(g[k] * 2.0 * th[k]), LR_STEP * 0.125f, bc);
         }
+        // the kept root, normalised so that it spans [0, 1]: piece ends
+        // b_t = float(C_t / C_R) of the running sums C of w = theta^2, made
+        // non-decreasing; piece t starts at b_{t-1} and its slope is the
+        // largest float w with b_{t-1} + w <= b_t in float arithmetic, so p0
+        // never decreases from the end of one piece to the start of the next
+        double w[RP], lane_w = 0.0;
 #pragma unroll
-        for (int k = 0; k < RP; ++k) rw[tid * RP + k] = best_th[k] * best_th[k];
-        if (tid == 0) {
-            loss_init_s = (float)first;
-            loss_best_s = (float)best;
+        for (int k = 0; k < RP; ++k) {
+            w[k] = (double)(best_th[k] * best_th[k]);
+            lane_w += w[k];
         }
-    }
-    __syncthreads();
-    // the kept root, normalised so that it spans [0, 1].  Piece t starts at
-    // c_t (rounded from the exact running sum) and its slope is the largest
-    // float w with c_t + w <= c_{t+1} in float arithmetic, so p0 never
-    // decreases from the end of one piece to the start of the next
-    if (tid == 0) {
-        double tot = 0.0;
-        for (int t = 0; t < LR_ROOT; ++t) tot += (double)rw[t];
+        double inc = lane_w;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const double o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+            if (tid >= d) inc += o;
+        }
+        const double tot = __shfl_sync(0xFFFFFFFFu, inc, 31);
         const double inv = tot > 0.0 ? 1.0 / tot : 0.0;
-        double c = 0.0;
-        float start = 0.f;
-        for (int t = 0; t < LR_ROOT; ++t) {
-            c += (double)rw[t];
-            const float next = t == LR_ROOT - 1 ? 1.f : (float)(c * inv);
-            float w = fmaxf(__fsub_rn(next, start), 0.f);
-            while (w > 0.f && __fadd_rn(start, w) > next) w = nextafterf(w, 0.f);
-            L.rcw[t] = make_float2(start, w);
-            start = next;
+        const double before = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+        double c = tid ? before : 0.0;
+        float b[RP];
+#pragma unroll
+        for (int k = 0; k < RP; ++k) {
+            c += w[k];
+            b[k] = (float)(c * inv);
+            if (k) b[k] = fmaxf(b[k], b[k - 1]);
         }
-        L.kmin = rm.kmin;
-        L.zscale = rm.zscale;
-        L.loss_init = loss_init_s;
-        L.loss_root = loss_best_s;
-        L.fitted = 1;
-        L.searches = searches ? 1u : 0u;
+        if (tid == 31) b[RP - 1] = fmaxf(b[RP - 1], 1.f);
+        float prev_end = b[RP - 1];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const float o = __shfl_up_sync(0xFFFFFFFFu, prev_end, d);
+            if (tid >= d) prev_end = fmaxf(prev_end, o);
+        }
+        prev_end = __shfl_up_sync(0xFFFFFFFFu, prev_end, 1);  // largest end of the earlier lanes
+        if (tid == 0) prev_end = 0.f;
+        float start = prev_end;
+#pragma unroll
+        for (int k = 0; k < RP; ++k) {
+            const float end = fmaxf(b[k], prev_end);
+            float wk = fmaxf(__fsub_rn(end, start), 0.f);
+            while (wk > 0.f && __fadd_rn(start, wk) > end) wk = nextafterf(wk, 0.f);
+            rcw[tid * RP + k] = make_float2(start, wk);
+            L.rcw[tid * RP + k] = make_float2(start, wk);
+            start = end;
+        }
+        if (tid == 0) {
+            L.kmin = rm.kmin;
+            L.zscale = rm.zscale;
+            L.loss_init = (float)first;
+            L.loss_root = (float)best;
+            L.fitted = 1;
+            L.searches = searches ? 1u : 0u;
+        }
     }
     __syncthreads();
     uint32_t* lf = lfirst + (size_t)sgi * (LR_LEAVES + 1);
     for (int l = tid; l <= LR_LEAVES; l += blockDim.x) lf[l] = m;
     __syncthreads();
     for (uint32_t i = tid; i < m; i += blockDim.x) {
-        const int l = leaf_of(root_p0<K>(L, smp[i]));
-        const int lp = i == 0 ? -1 : leaf_of(root_p0<K>(L, smp[i - 1]));
+        const int l = leaf_of(root_p0<K>(rm, rcw, smp[i]));
+        const int lp = i == 0 ? -1 : leaf_of(root_p0<K>(rm, rcw, smp[i - 1]));
         for (int q = lp + 1; q <= l; ++q) lf[q] = i;  // leaves lp+1..l start at i
     }
 }
