@@ -2,9 +2,8 @@
 // dealt into value slots by a monotone linear map of their offset from the
 // bucket's minimum, the slots are laid out by an exclusive scan of their
 // counts, the keys are dealt into their slots, and each slot that received
-// a few keys is put in order in place by the thread that scanned it; the keys
-// of a longer slot (repeated values, a local cluster) each count the keys of
-// their slot that go before them.
+// more than one key (a few keys at most) is put in order in place by the
+// thread that scanned it; the buffer is then the sorted bucket.
 //
 // A bucket that reaches the leaf stage holds the keys between two adjacent
 // quantile splitters, so its values are close to evenly spread over
@@ -25,8 +24,7 @@
 
 namespace s512 {
 
-constexpr uint32_t SLOT_MAX_RUN = 32;  // largest slot the slot sort takes
-constexpr uint32_t SLOT_OWNER_MAX = 4; // slots up to this many keys are put in order by one thread
+constexpr uint32_t SLOT_MAX_RUN = 32;  // largest slot put in order by one thread
 constexpr uint32_t SLOT_SUMSQ = 4;     // in-slot ordering work (sum of squared counts) allowed per key
 
 // Monotone map from a key in [lo, hi] to a slot in [0, nslots): the offset
@@ -67,15 +65,14 @@ struct SlotRed {
 };
 
 // Shared memory of block_slot_sort for a block of THREADS x IPT keys: the
-// key buffer (padded for the block sort when that runs inline, INLINE), the
-// counters, and one bit per key position that marks the positions of long
-// slots (ranked key by key).
+// key buffer (padded for the block sort when that runs inline, INLINE) and
+// the counters.
 template <typename K, int THREADS, int IPT, bool INLINE = true>
 struct SlotSmem {
     static constexpr uint32_t S = (uint32_t)THREADS * IPT;
     static constexpr size_t keys_bytes = ((size_t)(INLINE ? padded_len(S) : S) * sizeof(K) + 15) & ~(size_t)15;
     static constexpr size_t ctr_bytes = (size_t)S * sizeof(uint32_t);
-    static constexpr size_t bytes = keys_bytes + ctr_bytes + (size_t)S / 8;
+    static constexpr size_t bytes = keys_bytes + ctr_bytes;
 };
 
 // Sort the c <= THREADS*IPT keys held striped in key[] (element
@@ -100,7 +97,6 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
     using SM = SlotSmem<K, THREADS, IPT, INLINE_FALLBACK>;
     K* s = reinterpret_cast<K*>(smem);
     uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes);
-    uint32_t* longpos = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes + SM::ctr_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
     // 1. bounds of the bucket; counters zeroed
@@ -115,7 +111,6 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
 #pragma unroll
     for (int r = 0; r < IPT; r += 4)
         *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = make_uint4(0u, 0u, 0u, 0u);
-    for (uint32_t w = tid; w < S / 32; w += THREADS) longpos[w] = 0u;
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
         lo = kmin(lo, shfl_xor(lo, d));
@@ -216,22 +211,12 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
         refill();
         __syncthreads();
         // 5. the keys of a slot of several are in dealing order: the thread
-        //    that scanned a short slot puts them in key order, in place; a
-        //    long slot only marks its positions, and its keys rank
-        //    themselves in step 6
+        //    that scanned the slot puts them in key order, in place
         for (uint32_t bits = mbits; bits; bits &= bits - 1) {
-            const uint32_t r = (uint32_t)(__ffs(bits) - 1);
-            const uint32_t j = tid * IPT + r;
+            const uint32_t j = tid * IPT + (uint32_t)(__ffs(bits) - 1);
             const uint32_t a = j ? ctr[j - 1] : 0u;
             const uint32_t e = ctr[j];
-            if (e - a > SLOT_OWNER_MAX) {
-                for (uint32_t q = a; q < e; q = (q | 31u) + 1u) {
-                    const uint32_t hi = min(e, (q | 31u) + 1u);
-                    const uint32_t n = hi - q;
-                    const uint32_t m = (n == 32u ? 0xFFFFFFFFu : ((1u << n) - 1u)) << (q & 31u);
-                    atomicOr(&longpos[q >> 5], m);
-                }
-            } else if (e - a == 2) {
+            if (e - a == 2) {
                 const K x0 = s[a], x1 = s[a + 1];
                 if (x1 < x0) {
                     s[a] = x1;
@@ -251,24 +236,8 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
             }
         }
         __syncthreads();
-        // 6. a key of a short slot is in its final place; a key of a long one
-        //    counts the keys of its slot that go before it
-        for (uint32_t p = tid; p < c; p += THREADS) {
-            const K x = s[p];
-            if (!((longpos[p >> 5] >> (p & 31)) & 1u)) {
-                store(p, x);
-                continue;
-            }
-            const uint32_t j = f(x);
-            const uint32_t a = j ? ctr[j - 1] : 0u;
-            const uint32_t e = ctr[j];
-            uint32_t rank = a;
-            for (uint32_t q = a; q < e; ++q) {
-                const K y = s[q];
-                rank += (y < x || (y == x && q < p)) ? 1u : 0u;
-            }
-            store(rank, x);
-        }
+        // 6. every key is in its final place
+        for (uint32_t p = tid; p < c; p += THREADS) store(p, s[p]);
     } else if constexpr (INLINE_FALLBACK) {
         // uneven spread: bitonic leaves + merge path on the same keys
 #pragma unroll
