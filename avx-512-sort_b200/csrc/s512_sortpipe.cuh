@@ -19,10 +19,11 @@
 //     segment is written into a region whose capacity comes from the sample
 //     (a 6-sigma bound); a bucket that outgrows it is reported and the level
 //     is redone with exact counts;
-//   * buckets at most a leaf's capacity are sorted by the bitonic networks of
-//     s512_bitonic.cuh (one warp or one block per bucket, by size class) and
-//     written to their final place; larger buckets become the segments of the
-//     next partition level.
+//   * buckets at most a leaf's capacity are sorted in shared memory (one warp
+//     and the bitonic networks of s512_bitonic.cuh up to 256 keys, one block
+//     and the slot sort of s512_slotsort.cuh above, by size class) and written
+//     to their final place; larger buckets become the segments of the next
+//     partition level.
 #pragma once
 
 #include <cstddef>

@@ -1,8 +1,9 @@
-"""The decoupled look-back protocol of the partition pass, simulated with host
-threads (no GPU): tiles take chain positions in the order they start, publish
-their aggregate, walk back to the nearest inclusive count with a bounded wait,
-and publish their inclusive count.  The prefixes must equal a serial scan, and
-a tile that never publishes must make its successors time out, not hang."""
+"""The decoupled look-back protocol of the two-way partition behind
+Partition512 (s512_partition2.cuh), simulated with host threads (no GPU):
+tiles take chain positions in the order they start, publish their aggregate,
+walk back to the nearest inclusive count with a bounded wait, and publish
+their inclusive count.  The prefixes must equal a serial scan, and a tile that
+never publishes must make its successors time out, not hang."""
 import random
 import threading
 
