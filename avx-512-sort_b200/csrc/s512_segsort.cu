@@ -167,12 +167,37 @@ static int launch_classes(DevCtx& C, int shape, Codec io, const SegLists& L, con
     return S512_OK;
 }
 
-// Segments longer than a block: the partition levels, from the device list.
+// Segments longer than a block: the partition levels, from the device list,
+// on the pool's helper stream and with that stream's own scratch pool, so
+// that these latency-bound launches (a read-back between levels) run beside
+// the class launches queued on st.  `ready` (recorded on st before those
+// launches) orders them after the caller's earlier work; st waits for them
+// at the end, also after an error.
 template <typename K, typename Codec>
-static int sort_big(DevCtx& C, Codec io, const SegLists& L, uint32_t n_big, uint64_t big_keys, cudaStream_t st,
-                    PhaseTimer& tm, s512_stats& S) {
+static int sort_big_beside(DevCtx& C, Codec io, const SegLists& L, uint32_t n_big, uint64_t big_keys,
+                           cudaStream_t st, cudaEvent_t ready, s512_stats& S) {
     if (n_big == 0) return S512_OK;
-    return run_levels<K, Codec, Codec>(C, io, io, L.big, n_big, big_keys, st, tm, S, false);
+    cudaStream_t hs = C.copy_stream;
+    S512_CUDA_TRY(cudaStreamWaitEvent(hs, ready, 0));
+    int rc = S512_OK;
+    DevCtx* H = current_ctx(&rc, hs);
+    if (H) {
+        CallGuard guard(H, hs);
+        PhaseTimer tm(hs, false);
+        rc = run_levels<K, Codec, Codec>(*H, io, io, L.big, n_big, big_keys, hs, tm, S, false);
+    }
+    S512_CUDA_TRY(cudaEventRecord(C.events[1], hs));
+    S512_CUDA_TRY(cudaStreamWaitEvent(st, C.events[1], 0));
+    return rc;
+}
+
+// The helper stream and two events when there are long segments; `ready` is
+// recorded on st at once.
+static int big_prologue(DevCtx& C, uint32_t n_big, cudaStream_t st) {
+    if (n_big == 0) return S512_OK;
+    S512_CUDA_TRY(C.copy_resources(2));
+    S512_CUDA_TRY(cudaEventRecord(C.events[0], st));
+    return S512_OK;
 }
 
 // The whole batch on the device: classify, the class launches, long segments.
@@ -195,10 +220,12 @@ static int segsort_device(DevCtx& C, Codec io, const size_t* d_off, size_t nseg,
     S512_CUDA_TRY(cudaStreamSynchronize(st));
     const SegCtl counts = *h;
     S.kernel_launches += 1;
+    rc = big_prologue(C, counts.n_big, st);
+    if (rc) return rc;
     rc = launch_classes<Codec>(C, shape, io, L, counts, st, &S.kernel_launches);
     if (rc) return rc;
     const int t1 = tm.mark();
-    rc = sort_big<K, Codec>(C, io, L, counts.n_big, counts.big_keys, st, tm, S);
+    rc = sort_big_beside<K, Codec>(C, io, L, counts.n_big, counts.big_keys, st, C.events.empty() ? nullptr : C.events[0], S);
     if (rc) return rc;
     const int t2 = tm.mark();
     if (tm.on()) {
@@ -292,13 +319,14 @@ static int tune_dtype(DevCtx& C, int dt, Codec io, uint64_t total, const size_t*
                 cudaMemcpyAsync(&h, L.ctl, sizeof(SegCtl), cudaMemcpyDeviceToHost, st);
                 cudaStreamSynchronize(st);
                 uint32_t launches = 0;
-                rc = launch_classes<Codec>(C, shape, io, L, h, st, &launches);
+                rc = big_prologue(C, h.n_big, st);
+                if (!rc) rc = launch_classes<Codec>(C, shape, io, L, h, st, &launches);
             }
             if (!rc) {
-                PhaseTimer tm(st, false);
                 s512_stats S;
                 memset(&S, 0, sizeof(S));
-                rc = sort_big<K, Codec>(C, io, L, h.n_big, h.big_keys, st, tm, S);
+                rc = sort_big_beside<K, Codec>(C, io, L, h.n_big, h.big_keys, st,
+                                               C.events.empty() ? nullptr : C.events[0], S);
             }
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
@@ -488,17 +516,19 @@ int s512_segsort_plan_launch(s512_segsort_plan* plan, void* stream) {
     CallGuard guard(C, st);
     s512_stats& S = thread_stats();
     memset(&S, 0, sizeof(S));
+    const uint32_t nb = p->counts.n_big;
+    int rc = big_prologue(*C, nb, st);
+    if (rc) return rc;
     S512_CUDA_TRY(cudaGraphLaunch(p->exec, st));
     S.kernel_launches = p->launches;
-    if (p->counts.n_big) {
-        PhaseTimer tm(st, false);
+    if (nb) {
         const SegLists L = plan_lists(p);
-        const uint32_t nb = p->counts.n_big;
         const uint64_t bk = p->counts.big_keys;
-        int rc;
-        if (p->dt == DT_I32) rc = sort_big<uint32_t>(*C, make_i32(p->keys, p->values), L, nb, bk, st, tm, S);
-        else if (p->dt == DT_F64) rc = sort_big<uint64_t>(*C, make_f64(p->keys, p->values), L, nb, bk, st, tm, S);
-        else rc = sort_big<uint64_t>(*C, make_kv(p->keys, p->values), L, nb, bk, st, tm, S);
+        cudaEvent_t ready = C->events[0];
+        if (p->dt == DT_I32) rc = sort_big_beside<uint32_t>(*C, make_i32(p->keys, p->values), L, nb, bk, st, ready, S);
+        else if (p->dt == DT_F64)
+            rc = sort_big_beside<uint64_t>(*C, make_f64(p->keys, p->values), L, nb, bk, st, ready, S);
+        else rc = sort_big_beside<uint64_t>(*C, make_kv(p->keys, p->values), L, nb, bk, st, ready, S);
         if (rc) return rc;
     }
     guard.finish();
