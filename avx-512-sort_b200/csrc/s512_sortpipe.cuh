@@ -930,17 +930,80 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
     }
     const uint64_t c = (b < (int)nbk) ? a.bucket_counts[(size_t)s * NB + b] : 0ull;
     const uint64_t excl = block_exclusive_scan_first<NB, uint64_t>(c, wtot64, (uint64_t*)nullptr);
-    if (c == 0) return;
-    atomicMax(&a.ctl->max_bucket, (uint32_t)(c > 0xFFFFFFFFull ? 0xFFFFFFFFull : c));
-    atomicAdd(&a.ctl->nonempty, 1u);
-    atomicAdd((unsigned long long*)&a.ctl->level_keys, (unsigned long long)c);
-    atomicAdd(&a.ctl->bucket_sq, (double)c * (double)c);
+    // what the bucket becomes: a copy (equality bucket or single key, in
+    // chunks), a leaf of some class, or a segment of the next level
+    constexpr int LIST_NEXT = NCLASS + 1;  // lists 0..NCLASS-1 leaves, NCLASS copies, NCLASS+1 next level
+    __shared__ uint32_t list_n[NCLASS + 2], list_base[NCLASS + 2];
+    __shared__ uint32_t st_max, st_nonempty;
+    __shared__ unsigned long long st_keys, st_next_keys;
+    __shared__ double st_sq;
+    if (b < NCLASS + 2) list_n[b] = 0;
+    if (b == 0) {
+        st_max = 0;
+        st_nonempty = 0;
+        st_keys = 0;
+        st_next_keys = 0;
+        st_sq = 0.0;
+    }
+    __syncthreads();
+    const bool is_eq = (bucket_eq[b >> 5] >> (b & 31)) & 1u;
+    int list = -1;
+    uint32_t nslots = 0;
+    if (c > 0) {
+        if (is_eq || c == 1) {
+            list = CLS_COPY;
+            nslots = (uint32_t)((c + COPY_CHUNK - 1) / COPY_CHUNK);
+        } else if (c <= leaf_max(a.key_bytes)) {
+            list = class_of(a.key_bytes, (uint32_t)c);
+            nslots = 1;
+        } else {
+            list = LIST_NEXT;
+            nslots = 1;
+        }
+    }
+    // the level's statistics and the list slots, gathered in the block: one
+    // global atomic per block and counter instead of one per bucket
+    const uint32_t local = list >= 0 ? atomicAdd(&list_n[list], nslots) : 0u;
+    {
+        uint32_t mx = (uint32_t)(c > 0xFFFFFFFFull ? 0xFFFFFFFFull : c), ne = c > 0 ? 1u : 0u;
+        unsigned long long keys = c, nk = list == LIST_NEXT ? c : 0ull;
+        double sq = (double)c * (double)c;
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, d));
+            ne += __shfl_xor_sync(0xFFFFFFFFu, ne, d);
+            keys += __shfl_xor_sync(0xFFFFFFFFu, keys, d);
+            nk += __shfl_xor_sync(0xFFFFFFFFu, nk, d);
+            sq += __shfl_xor_sync(0xFFFFFFFFu, sq, d);
+        }
+        if ((b & 31) == 0 && ne) {
+            atomicMax(&st_max, mx);
+            atomicAdd(&st_nonempty, ne);
+            atomicAdd(&st_keys, keys);
+            atomicAdd(&st_next_keys, nk);
+            atomicAdd(&st_sq, sq);
+        }
+    }
+    __syncthreads();
+    if (b < NCLASS + 2 && list_n[b]) {
+        unsigned int* ctr = b == LIST_NEXT ? &a.ctl->n_next : &a.ctl->n_items[b];
+        list_base[b] = atomicAdd(ctr, list_n[b]);
+    }
+    if (b == 0 && st_nonempty) {
+        atomicMax(&a.ctl->max_bucket, st_max);
+        atomicAdd(&a.ctl->nonempty, st_nonempty);
+        atomicAdd((unsigned long long*)&a.ctl->level_keys, st_keys);
+        atomicAdd(&a.ctl->bucket_sq, st_sq);
+        if (st_next_keys) atomicAdd((unsigned long long*)&a.ctl->next_keys, st_next_keys);
+    }
+    __syncthreads();
+    if (list < 0) return;
     const K* src = a.level_out + sd.out_base + region_off[b];
     const uint64_t dst = sd.final_off + excl;
-    const bool is_eq = (bucket_eq[b >> 5] >> (b & 31)) & 1u;
-    if (is_eq || c == 1) {
-        for (uint64_t o = 0; o < c; o += COPY_CHUNK) {
-            const uint32_t slot = atomicAdd(&a.ctl->n_items[CLS_COPY], 1u);
+    const uint32_t first = list_base[list] + local;
+    if (list == CLS_COPY) {
+        uint32_t slot = first;
+        for (uint64_t o = 0; o < c; o += COPY_CHUNK, ++slot) {
             if (slot < a.item_cap) {
                 LeafItem<K> it;
                 it.src = src + o;
@@ -952,22 +1015,19 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
                 raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
             }
         }
-    } else if (c <= leaf_max(a.key_bytes)) {
-        const int cls = class_of(a.key_bytes, (uint32_t)c);
-        const uint32_t slot = atomicAdd(&a.ctl->n_items[cls], 1u);
-        if (slot < a.item_cap) {
+    } else if (list < NCLASS) {
+        if (first < a.item_cap) {
             LeafItem<K> it;
             it.src = src;
             it.dst = dst;
             it.count = (uint32_t)c;
             it.pad_ = 0;
-            a.items[cls][slot] = it;
+            a.items[list][first] = it;
         } else {
             raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
         }
     } else {
-        const uint32_t slot = atomicAdd(&a.ctl->n_next, 1u);
-        if (slot < a.next_cap) {
+        if (first < a.next_cap) {
             SegDesc n;
             n.in_off = sd.out_base + region_off[b];
             n.count = c;
@@ -975,8 +1035,7 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
             n.out_base = 0;
             n.tile_start = 0;
             n.ntiles = 0;
-            a.next[slot] = n;
-            atomicAdd((unsigned long long*)&a.ctl->next_keys, (unsigned long long)c);
+            a.next[first] = n;
         } else {
             raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
         }
