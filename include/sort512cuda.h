@@ -191,7 +191,8 @@ S512_API int s512_sort_omp_merge_f64(double* data, size_t n, int nparts, int fla
  *     arrays (sort512perf.cpp:612-709, timeSmall).  Segments of up to 256
  *     keys are sorted one per warp, longer ones one per block of the smallest
  *     size class that holds them (1K, 2K, 4K, 8K, 16K keys), one persistent
- *     launch per class; longer ones run the partition levels. */
+ *     launch per class; longer ones run the partition levels, on a helper
+ *     stream beside the class launches (the call's stream waits for them). */
 S512_API int s512_segsort_i32(int* data, const size_t* offsets, size_t nseg, int flags, void* stream);
 S512_API int s512_segsort_f64(double* data, const size_t* offsets, size_t nseg, int flags, void* stream);
 S512_API int s512_segsort_kv_i32(int* keys, int* values, const size_t* offsets, size_t nseg, int flags,
@@ -211,10 +212,10 @@ S512_API int s512_segsort_tune(int dtype, const size_t* d_offsets, size_t nseg, 
 
 /* A segmented sort captured in a CUDA graph for repeated use on the same
  * device buffers and layout: classification happens once at creation; each
- * launch replays the captured class launches (and runs the partition levels
- * for segments longer than the largest class, which are not captured: their
- * level structure depends on the data).  values is used by S512_DTYPE_KV_I32
- * only. */
+ * launch replays the captured class launches and, beside them on a helper
+ * stream, runs the partition levels for segments longer than the largest
+ * class (not captured: their level structure depends on the data; the launch
+ * stream waits for them).  values is used by S512_DTYPE_KV_I32 only. */
 typedef struct s512_segsort_plan s512_segsort_plan;
 S512_API int s512_segsort_plan_create(s512_segsort_plan** plan, int dtype, void* keys, void* values,
                                       const size_t* d_offsets, size_t nseg, void* stream);
