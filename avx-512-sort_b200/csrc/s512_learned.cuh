@@ -578,7 +578,7 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     __shared__ uint32_t first_heavy[NB];
     __shared__ uint32_t wt32[32];
     __shared__ uint64_t wt64[32];
-    __shared__ uint32_t max_s, nonempty_s, tot_ids_s, sorted_s;
+    __shared__ uint32_t max_s, tot_ids_s, sorted_s;
     __shared__ float loss_s, top_w[NB / 32];
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -592,7 +592,6 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     const K* smp = samples + (size_t)sgi * SAMPLE_N;
     if (tid == 0) {
         max_s = 0;
-        nonempty_s = 0;
         sorted_s = 0;
         loss_s = 0.f;
     }
@@ -666,7 +665,6 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     const uint32_t c = hist[tid];
     if (c && !((L.bucket_eq[tid >> 5] >> (tid & 31)) & 1u)) {
         atomicMax(&max_s, c);
-        atomicAdd(&nonempty_s, 1u);
         atomicAdd(&sorted_s, c);
     }
     const double scale = (double)sd.count / (double)m;
@@ -695,7 +693,10 @@ __global__ void __launch_bounds__(NB) learned_finish_kernel(const K* __restrict_
     }
     __syncthreads();
     if (tid == 0) {
-        const float mean = nonempty_s ? (float)sorted_s / (float)nonempty_s : 1.f;
+        // against the mean the model aims at: the sorted samples spread over
+        // all nmodel model buckets (a model that sends the sample to a few
+        // buckets is unbalanced, however even those few are)
+        const float mean = sorted_s ? (float)sorted_s / (float)L.nmodel : 1.f;
         L.max_over_mean = (float)max_s / mean;
         L.balanced = (L.max_over_mean <= max_imbalance && L.nbuckets <= (uint32_t)NB) ? 1u : 0u;
         L.ok = (L.balanced && L.searches) ? 1u : 0u;
