@@ -154,6 +154,7 @@ struct Level {
     const uint32_t* ntiles_dev; // levels >= 1
     uint32_t ntiles_bound;
     K* out;
+    uint64_t junk;              // offset in out of JUNK_KEYS keys past every region (overflow writes)
     bool aligned;               // every tile starts 16-byte aligned (bulk copies allowed)
 };
 
@@ -226,6 +227,7 @@ static int run_level(DevCtx& C, Level<K, InCodec>& L, int level, UserOut uout, s
     pa.tile_seg = L.tile_seg;
     pa.splits = splits;
     pa.out = L.out;
+    pa.junk = L.junk;
     pa.fill = (unsigned long long*)counts;
     pa.ctl = ctl;
     pa.ntiles = L.ntiles_host;
@@ -398,9 +400,11 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
     // needs the sum over its segments of region_bound(count) rounded to 16
     // (prepare_level_kernel lays the segments out that way).
     K* T[2];
+    // (plus JUNK_KEYS at the end, where a bucket that overflows its region
+    // writes that tile's keys: the level is then redone)
     const size_t need0 = single ? region_bound(keys0) + 64
                                 : 2 * keys0 + keys0 / 100 + (size_t)nsegs0 * (4096 + 16) + 64;
-    T[0] = (K*)C.get("T0", need0 * KB);
+    T[0] = (K*)C.get("T0", (need0 + JUNK_KEYS) * KB);
     T[1] = nullptr;
     LevelCtl* ctls = (LevelCtl*)C.get("ctl", 2 * sizeof(LevelCtl));
     LevelCtl* host_ctl = (LevelCtl*)C.host_pinned(sizeof(LevelCtl));
@@ -416,6 +420,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
     L0.segs = segs0;
     L0.nsegs = nsegs0;
     L0.out = T[0];
+    L0.junk = need0;
     if (single) {
         L0.tile_seg = nullptr;
         L0.ntiles_host = (uint32_t)((keys0 + TILE_ONE - 1) / TILE_ONE);
@@ -461,7 +466,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         // grow (never shrink) this level's output buffer; its old contents
         // were consumed two levels ago
         const size_t need = 2 * next_keys + next_keys / 100 + (size_t)nsegs * (4096 + 16) + 64;
-        T[level & 1] = (K*)C.get((level & 1) ? "T1" : "T0", need * KB);
+        T[level & 1] = (K*)C.get((level & 1) ? "T1" : "T0", (need + JUNK_KEYS) * KB);
         K* out_buf = T[level & 1];
         if (!out_buf) return S512_ERR_ALLOC;
         const uint32_t ntiles_bound = (uint32_t)(next_keys / TILE) + nsegs + 1;
@@ -484,6 +489,7 @@ static int run_levels(DevCtx& C, UserIn uin, UserOut uout, SegDesc* segs0, uint3
         Ln.ntiles_dev = &tctl->ntiles_next;
         Ln.ntiles_bound = ntiles_bound;
         Ln.out = out_buf;
+        Ln.junk = need;
         Ln.aligned = true;
         // the tile count lives in tctl, so the level's own control block is the other one
         rc = run_level<K, Raw<K>, UserOut>(C, Ln, level, uout, keys0, st, lctl, tctl, nxt, next_cap, tm, S,

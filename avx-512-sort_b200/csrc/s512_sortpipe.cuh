@@ -468,7 +468,10 @@ constexpr int SEG_SMEM = 256;  // segment tables up to this size are searched in
 // segment takes short ones (a finer split of the last tiles among blocks).
 constexpr uint32_t CLAIM_GROUP_ONE_SEG = 4;
 constexpr uint32_t CLAIM_GROUP_MANY_SEGS = 16;
-constexpr uint64_t GDELTA_DROP = ~0ull;  // write offset of a bucket that overflowed its region
+// Keys past the regions of a level buffer where a bucket that overflowed its
+// region writes its keys of the tile (at most a tile's worth; tiles race
+// there harmlessly: the level is redone with exact counts).
+constexpr uint64_t JUNK_KEYS = 8192;
 
 template <typename K>
 struct PartArgs {
@@ -477,6 +480,7 @@ struct PartArgs {
     const uint32_t* tile_seg;     // global tile -> segment (nullptr: single segment 0)
     const SplitSet<K>* splits;
     K* out;                       // level output buffer
+    uint64_t junk;                // offset in out of the JUNK_KEYS overflow area
     unsigned long long* fill;     // nsegs * NB fill counters (zeroed); end as the bucket sizes
     LevelCtl* ctl;
     uint32_t ntiles;              // end of the launch's tiles (used when ntiles_dev is null)
@@ -536,6 +540,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
     constexpr int ESZ = InCodec::ESZ;
     constexpr int NARR = InCodec::NARR;
     static_assert(TILE < (1 << 24), "rank and bucket share a 32-bit word");
+    static_assert(TILE <= (int)JUNK_KEYS, "an overflowed bucket's keys of a tile fit the overflow area");
     const int tid = threadIdx.x;
     const uint32_t ntiles = a.ntiles_dev ? *a.ntiles_dev : a.ntiles;
     const bool small_tab = a.tile_seg && a.nsegs <= (uint32_t)SEG_SMEM;
@@ -799,20 +804,20 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) partition_kernel(Part
                 const bool ovf = !data_ok || end > sm.region_cap[tid];
                 if (ovf && h) raise_error(&a.ctl->err, data_ok ? DEV_ERR_OVERFLOW : DEV_ERR_TIMEOUT);
                 sm.gdelta[tid] =
-                    ovf ? GDELTA_DROP : sm.sd.out_base + sm.region_off[tid] + off - (uint64_t)sm.loc[tid];
+                    (ovf ? a.junk : sm.sd.out_base + sm.region_off[tid] + off) - (uint64_t)sm.loc[tid];
                 sm.hist[tid] = 0;  // (next used after barrier (3))
             }
             if (tid == 0 && !data_ok) sm.abort = 1;
             __syncthreads();  // (3) staging complete
 
-            // D. coalesced write-out (an overflowed bucket's keys are dropped:
-            // the level is redone)
+            // D. coalesced write-out (an overflowed bucket's keys go to the
+            // overflow area past the regions: the level is redone)
 #pragma unroll
             for (int r = 0; r < IPT; ++r) {
                 const uint32_t i = (uint32_t)(r * THREADS + tid);
                 if (FULL || i < cnt) {
                     const uint64_t g = sm.gdelta[sm.bkt[i]];
-                    if (g != GDELTA_DROP) a.out[g + i] = stage[i];
+                    a.out[g + i] = stage[i];
                 }
             }
         }
