@@ -8,14 +8,14 @@
 // about six times the data for the array plus the level buffers) is sorted
 // here as:
 //   1. runs: consecutive pieces of m keys are copied in, sorted on the device
-//      and copied out to a pinned staging array;
+//      and copied out to a pinned staging array, three pieces in flight;
 //   2. merge by exact rank: output piece j holds ranks [j*m, (j+1)*m).  For
 //      each boundary rank the host finds the boundary key by bisection over
 //      the encoded key range (counting keys <= a value with one binary search
 //      per run) and splits ties between runs in run order, which gives every
 //      run's cut exactly; piece j is then the runs' slices between two cuts,
 //      gathered to the device, sorted there and copied to its final place in
-//      the caller's array.
+//      the caller's array, again three pieces in flight.
 // Every piece holds at most m keys whatever the data (ties included), so the
 // device budget holds.  Keys cross PCIe twice each way.
 #pragma once
@@ -117,12 +117,20 @@ static size_t count_le(void* const* stage, size_t first, size_t len, uint64_t v,
     return lo;
 }
 
+// Pieces in flight: while one is sorted, the copies of the next ones in and of
+// the previous ones out run in both directions of PCIe.  Each has its own
+// stream and scratch pool (the caller's, then helper streams), and a piece
+// buffer is reused three pieces later, after its copy out on the same stream.
+constexpr int STREAM_INFLIGHT = 3;
+
 template <typename ST>
 static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream_t st) {
     using K = typename ST::K;
     constexpr int NA = ST::NARR;
+    constexpr int F = STREAM_INFLIGHT;
     const size_t esz = ST::ESZ;
-    const size_t m = stream_piece_keys(esz * NA);
+    size_t m = stream_piece_keys(esz * NA) / F;
+    m = m < 65536 ? 65536 : (m & ~(size_t)4095);
     const size_t nruns = (n + m - 1) / m;
 
     struct Pinned {
@@ -132,29 +140,65 @@ static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream
                 if (q) cudaFreeHost(q);
         }
     } stage;
-    void* d[2] = {nullptr, nullptr};
+    // streams and pools: S[0] the caller's (pool C, already held), S[1] and
+    // S[2] the copy streams of the pools before them
+    cudaStream_t S[F];
+    DevCtx* P[F];
+    S[0] = st;
+    P[0] = &C;
+    for (int b = 1; b < F; ++b) {
+        S512_CUDA_TRY(P[b - 1]->copy_resources(1));
+        S[b] = P[b - 1]->copy_stream;
+        int rc = S512_OK;
+        P[b] = current_ctx(&rc, S[b]);
+        if (!P[b]) return rc;
+    }
+    static_assert(F == 3, "one guard per helper pool below");
+    CallGuard g1(P[1], S[1]), g2(P[2], S[2]);
+    // every return waits for all F streams first: their copies and sorts use
+    // the pools' buffers and the staging arrays (freed after this)
+    struct Drain {
+        cudaStream_t* s;
+        ~Drain() {
+            for (int b = 0; b < F; ++b) cudaStreamSynchronize(s[b]);
+        }
+    } drain{S};
+    void* d[F][2] = {};
     for (int k = 0; k < NA; ++k) {
         if (cudaMallocHost(&stage.p[k], n * esz) != cudaSuccess) {
             cudaGetLastError();
             set_error("cudaMallocHost of %zu bytes for the streamed sort failed", n * esz);
             return S512_ERR_ALLOC;
         }
-        d[k] = C.get(k ? "stream_piece1" : "stream_piece0", m * esz);
-        if (!d[k]) return S512_ERR_ALLOC;
+        for (int b = 0; b < F; ++b) {
+            d[b][k] = P[b]->get(k ? "stream_piece1" : "stream_piece0", m * esz);
+            if (!d[b][k]) return S512_ERR_ALLOC;
+        }
     }
     auto at = [&](void* base, size_t i) { return static_cast<char*>(base) + i * esz; };
+    auto piece_len = [&](size_t r) { return (n - r * m) < m ? (n - r * m) : m; };
 
-    // 1. sorted runs of m elements into the staging arrays
-    for (size_t r = 0; r < nruns; ++r) {
-        const size_t off = r * m, len = (n - off) < m ? (n - off) : m;
+    // 1. sorted runs of m elements into the staging arrays; the inputs of the
+    //    next F-1 runs are queued before a run's sort (which waits on the host
+    //    between its levels)
+    auto run_in = [&](size_t r) -> int {
+        const int b = (int)(r % F);
         for (int k = 0; k < NA; ++k)
-            S512_CUDA_TRY(cudaMemcpyAsync(d[k], at(host[k], off), len * esz, cudaMemcpyHostToDevice, st));
-        int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
+            S512_CUDA_TRY(cudaMemcpyAsync(d[b][k], at(host[k], r * m), piece_len(r) * esz, cudaMemcpyHostToDevice,
+                                          S[b]));
+        return S512_OK;
+    };
+    for (size_t r = 0; r + 1 < F && r < nruns; ++r) S512_TRY_RC(run_in(r));
+    for (size_t r = 0; r < nruns; ++r) {
+        if (r + F - 1 < nruns) S512_TRY_RC(run_in(r + F - 1));
+        const int b = (int)(r % F);
+        int rc = sort_device<K>(*P[b], ST::codec(d[b]), ST::codec(d[b]), piece_len(r), S[b]);
         if (rc) return rc;
         for (int k = 0; k < NA; ++k)
-            S512_CUDA_TRY(cudaMemcpyAsync(at(stage.p[k], off), d[k], len * esz, cudaMemcpyDeviceToHost, st));
+            S512_CUDA_TRY(cudaMemcpyAsync(at(stage.p[k], r * m), d[b][k], piece_len(r) * esz,
+                                          cudaMemcpyDeviceToHost, S[b]));
     }
-    S512_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int b = 0; b < F; ++b) S512_CUDA_TRY(cudaStreamSynchronize(S[b]));
 
     auto run_len = [&](size_t r) { return (n - r * m) < m ? (n - r * m) : m; };
 
@@ -194,27 +238,36 @@ static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream
     }
 
     // 3. each output piece: gather its slices, sort, copy to its final place
-    for (size_t j = 0; j < nruns; ++j) {
+    //    (the gathers of the next F-1 pieces queued before a piece's sort)
+    auto piece_in = [&](size_t j) -> int {
+        const int b = (int)(j % F);
         size_t len = 0;
         for (size_t r = 0; r < nruns; ++r) {
-            const size_t a = cut[j][r], b = cut[j + 1][r];
-            if (b > a) {
+            const size_t a = cut[j][r], e = cut[j + 1][r];
+            if (e > a) {
                 for (int k = 0; k < NA; ++k)
-                    S512_CUDA_TRY(cudaMemcpyAsync(at(d[k], len), at(stage.p[k], r * m + a), (b - a) * esz,
-                                                  cudaMemcpyHostToDevice, st));
-                len += b - a;
+                    S512_CUDA_TRY(cudaMemcpyAsync(at(d[b][k], len), at(stage.p[k], r * m + a), (e - a) * esz,
+                                                  cudaMemcpyHostToDevice, S[b]));
+                len += e - a;
             }
         }
         if (len != run_len(j)) {
             set_error("streamed sort: piece %zu holds %zu keys, expected %zu", j, len, run_len(j));
             return S512_ERR_INTERNAL;
         }
-        int rc = sort_device<K>(C, ST::codec(d), ST::codec(d), len, st);
+        return S512_OK;
+    };
+    for (size_t j = 0; j + 1 < F && j < nruns; ++j) S512_TRY_RC(piece_in(j));
+    for (size_t j = 0; j < nruns; ++j) {
+        if (j + F - 1 < nruns) S512_TRY_RC(piece_in(j + F - 1));
+        const int b = (int)(j % F);
+        int rc = sort_device<K>(*P[b], ST::codec(d[b]), ST::codec(d[b]), run_len(j), S[b]);
         if (rc) return rc;
         for (int k = 0; k < NA; ++k)
-            S512_CUDA_TRY(cudaMemcpyAsync(at(host[k], j * m), d[k], len * esz, cudaMemcpyDeviceToHost, st));
+            S512_CUDA_TRY(cudaMemcpyAsync(at(host[k], j * m), d[b][k], run_len(j) * esz, cudaMemcpyDeviceToHost,
+                                          S[b]));
     }
-    S512_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int b = 0; b < F; ++b) S512_CUDA_TRY(cudaStreamSynchronize(S[b]));
     return S512_OK;
 }
 
