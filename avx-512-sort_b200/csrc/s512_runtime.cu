@@ -67,6 +67,23 @@ void* DevCtx::get(const char* name, size_t bytes) {
     return p;
 }
 
+void* DevCtx::stage_pinned(int k, size_t bytes) {
+    if (stage_bytes[k] >= bytes) return stage[k];
+    if (stage[k]) {
+        cudaStreamSynchronize(stream);
+        cudaFreeHost(stage[k]);
+    }
+    stage[k] = nullptr;
+    stage_bytes[k] = 0;
+    if (cudaMallocHost(&stage[k], bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("cudaMallocHost of %zu bytes for the streamed sort failed", bytes);
+        return nullptr;
+    }
+    stage_bytes[k] = bytes;
+    return stage[k];
+}
+
 void* DevCtx::host_pinned(size_t bytes) {
     if (pinned_bytes >= bytes) return pinned;
     if (pinned) {
@@ -90,6 +107,11 @@ void DevCtx::release_all() {
     if (pinned) cudaFreeHost(pinned);
     pinned = nullptr;
     pinned_bytes = 0;
+    for (int k = 0; k < 2; ++k) {
+        if (stage[k]) cudaFreeHost(stage[k]);
+        stage[k] = nullptr;
+        stage_bytes[k] = 0;
+    }
     for (auto e : events) cudaEventDestroy(e);
     events.clear();
     if (copy_stream) cudaStreamDestroy(copy_stream);

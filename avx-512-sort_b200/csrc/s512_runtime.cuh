@@ -87,12 +87,17 @@ struct DevCtx {
     std::map<std::string, std::pair<void*, size_t>> bufs;
     void* pinned = nullptr;          // small pinned host buffer for read-backs
     size_t pinned_bytes = 0;
+    void* stage[2] = {nullptr, nullptr};  // streamed sorts: page-locked staging arrays (grow-only)
+    size_t stage_bytes[2] = {0, 0};
     cudaStream_t copy_stream = nullptr;  // host-pointer sorts: input copies beside the sort
     std::vector<cudaEvent_t> events;     // host-pointer sorts: chunk arrivals (+1: call start)
 
     // grow-only named scratch buffer
     void* get(const char* name, size_t bytes);
     void* host_pinned(size_t bytes);
+    // page-locked staging array k (0 or 1) of at least `bytes`, kept for the
+    // next call like the device scratch (page-locking is slow)
+    void* stage_pinned(int k, size_t bytes);
     void release_all();
     // blocks for a persistent launch: SMs x resident blocks per SM
     int persistent_grid(const void* fn, int threads, size_t smem);

@@ -133,13 +133,9 @@ static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream
     m = m < 65536 ? 65536 : (m & ~(size_t)4095);
     const size_t nruns = (n + m - 1) / m;
 
-    struct Pinned {
+    struct {
         void* p[2] = {nullptr, nullptr};
-        ~Pinned() {
-            for (void* q : p)
-                if (q) cudaFreeHost(q);
-        }
-    } stage;
+    } stage;  // the pool's page-locked staging arrays
     // streams and pools: S[0] the caller's (pool C, already held), S[1] and
     // S[2] the copy streams of the pools before them
     cudaStream_t S[F];
@@ -156,7 +152,7 @@ static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream
     static_assert(F == 3, "one guard per helper pool below");
     CallGuard g1(P[1], S[1]), g2(P[2], S[2]);
     // every return waits for all F streams first: their copies and sorts use
-    // the pools' buffers and the staging arrays (freed after this)
+    // the pools' buffers and the staging arrays
     struct Drain {
         cudaStream_t* s;
         ~Drain() {
@@ -165,11 +161,8 @@ static int stream_sort_arrays(DevCtx& C, void* const* host, size_t n, cudaStream
     } drain{S};
     void* d[F][2] = {};
     for (int k = 0; k < NA; ++k) {
-        if (cudaMallocHost(&stage.p[k], n * esz) != cudaSuccess) {
-            cudaGetLastError();
-            set_error("cudaMallocHost of %zu bytes for the streamed sort failed", n * esz);
-            return S512_ERR_ALLOC;
-        }
+        stage.p[k] = C.stage_pinned(k, n * esz);
+        if (!stage.p[k]) return S512_ERR_ALLOC;
         for (int b = 0; b < F; ++b) {
             d[b][k] = P[b]->get(k ? "stream_piece1" : "stream_piece0", m * esz);
             if (!d[b][k]) return S512_ERR_ALLOC;

@@ -15,8 +15,9 @@
  *
  * Every operation is in place, like the reference.  Scratch memory comes from
  * one pool per (device, stream) that grows on demand and is kept until
- * s512_release_scratch() or process exit; calls on different streams use
- * different pools, so they may overlap on the device.
+ * s512_release_scratch() or process exit (the page-locked host staging array
+ * of a streamed sort, below, too); calls on different streams use different
+ * pools, so they may overlap on the device.
  *
  * Element types: int32 ("i32"), double ("f64") and int32 key + int32 value
  * pairs held in two arrays ("kv_i32").  Results:
