@@ -406,34 +406,6 @@ __device__ __forceinline__ uint32_t bucket_from_slot(uint32_t e, K x, bool has_e
     return range_b[j];
 }
 
-// The same bucket through the splitter lookup table: the key's slot gives the
-// unique splitters below it and the few that share its slot, which are
-// settled by comparisons with uniq[] (none for most keys).
-template <typename K>
-__device__ __forceinline__ uint32_t find_bucket_tab(const uint16_t* __restrict__ tab, const SlotMap<K>& f, K fhi,
-                                                    K x, bool has_eq, const K* __restrict__ uniq,
-                                                    const uint8_t* __restrict__ range_b,
-                                                    const uint8_t* __restrict__ eq_b,
-                                                    const uint32_t* __restrict__ eq_mask) {
-    const K xc = kmin(kmax(x, f.lo), fhi);
-    const uint32_t e = tab[f(xc)];
-    uint32_t lo = e & 0xFFu;
-    const uint32_t cnt = e >> 8;
-    if (cnt == 1) {  // one splitter shares the key's slot
-        lo += uniq[lo] < x ? 1u : 0u;
-    } else if (cnt > 1) {
-        uint32_t hi = lo + cnt;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (uniq[mid] < x) lo = mid + 1; else hi = mid;
-        }
-    }
-    const uint32_t j = lo;  // number of unique splitters < x
-    if (!has_eq) return j;
-    if (j < 255 && ((eq_mask[j >> 5] >> (j & 31)) & 1u) && uniq[j] == x) return eq_b[j];
-    return range_b[j];
-}
-
 }  // namespace s512
 
 #include "s512_learned.cuh"
