@@ -78,9 +78,7 @@ struct SlotSmem {
 // Sort the c <= THREADS*IPT keys held striped in key[] (element
 // r*THREADS + tid in key[r]; entries past c are ignored) into store(0..c).
 // `smem` holds SlotSmem<K,THREADS,IPT>::bytes; `red` is the block's reduction
-// scratch.  [klo, khi], when klo <= khi, bounds every key (the caller's
-// splitters): the bounds reduction is then skipped; slots are clamped to the
-// counters all the same.  refill() is called exactly once, as soon as key[] is no longer
+// scratch.  refill() is called exactly once, as soon as key[] is no longer
 // needed, so that the caller can start loading the next bucket into it while
 // this one is ranked and written.  Every thread of the block must call it; it
 // ends with a barrier, so the caller may reuse the shared memory right after.
@@ -92,7 +90,7 @@ struct SlotSmem {
 // the kernel keeps the slot path's register budget for the keys.
 template <typename K, int THREADS, int IPT, bool INLINE_FALLBACK, typename Store, typename Refill, typename Uneven>
 __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill refill, Uneven uneven,
-                                unsigned char* smem, SlotRed<K>& red, K klo = KeyMax<K>::value, K khi = K(0)) {
+                                unsigned char* smem, SlotRed<K>& red) {
     constexpr uint32_t S = (uint32_t)THREADS * IPT;
     constexpr int NW = THREADS / 32;
     static_assert(IPT % 4 == 0 && IPT <= 32, "counters are read four at a time, slot bits in one word");
@@ -101,41 +99,34 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
     uint32_t* ctr = reinterpret_cast<uint32_t*>(smem + SM::keys_bytes);
     const unsigned tid = threadIdx.x, lane = lane_id(), warp = tid >> 5;
 
-    // 1. bounds of the bucket (given by the caller when its splitters bound
-    //    the keys, klo <= khi); counters zeroed
-    K lo = klo, hi = khi;
+    // 1. bounds of the bucket; counters zeroed
+    K lo = KeyMax<K>::value, hi = K(0);
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+        if ((uint32_t)r * THREADS + tid < c) {
+            lo = kmin(lo, key[r]);
+            hi = kmax(hi, key[r]);
+        }
+    }
 #pragma unroll
     for (int r = 0; r < IPT; r += 4)
         *reinterpret_cast<uint4*>(&ctr[tid * IPT + r]) = make_uint4(0u, 0u, 0u, 0u);
-    if (klo <= khi) {
-        __syncthreads();
-    } else {
-        lo = KeyMax<K>::value;
-        hi = K(0);
 #pragma unroll
-        for (int r = 0; r < IPT; ++r) {
-            if ((uint32_t)r * THREADS + tid < c) {
-                lo = kmin(lo, key[r]);
-                hi = kmax(hi, key[r]);
-            }
-        }
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = kmin(lo, shfl_xor(lo, d));
+        hi = kmax(hi, shfl_xor(hi, d));
+    }
+    if (lane == 0) {
+        red.wlo[warp] = lo;
+        red.whi[warp] = hi;
+    }
+    __syncthreads();
+    lo = lane < (unsigned)NW ? red.wlo[lane] : KeyMax<K>::value;
+    hi = lane < (unsigned)NW ? red.whi[lane] : K(0);
 #pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            lo = kmin(lo, shfl_xor(lo, d));
-            hi = kmax(hi, shfl_xor(hi, d));
-        }
-        if (lane == 0) {
-            red.wlo[warp] = lo;
-            red.whi[warp] = hi;
-        }
-        __syncthreads();
-        lo = lane < (unsigned)NW ? red.wlo[lane] : KeyMax<K>::value;
-        hi = lane < (unsigned)NW ? red.whi[lane] : K(0);
-#pragma unroll
-        for (int d = 16; d > 0; d >>= 1) {
-            lo = kmin(lo, shfl_xor(lo, d));
-            hi = kmax(hi, shfl_xor(hi, d));
-        }
+    for (int d = 16; d > 0; d >>= 1) {
+        lo = kmin(lo, shfl_xor(lo, d));
+        hi = kmax(hi, shfl_xor(hi, d));
     }
 
     if (lo == hi) {  // every key equal: already in order
@@ -153,7 +144,7 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
     const SlotMap<K> f = make_slot_map<K>(lo, hi, S);
 #pragma unroll
     for (int r = 0; r < IPT; ++r) {
-        if ((uint32_t)r * THREADS + tid < c) atomicAdd(&ctr[min(f(key[r]), S - 1)], 1u);
+        if ((uint32_t)r * THREADS + tid < c) atomicAdd(&ctr[f(key[r])], 1u);
     }
     __syncthreads();
 
@@ -215,7 +206,7 @@ __device__ bool block_slot_sort(K (&key)[IPT], uint32_t c, Store store, Refill r
         // 4. deal the keys into their slots; afterwards ctr[j] is the end of slot j
 #pragma unroll
         for (int r = 0; r < IPT; ++r) {
-            if ((uint32_t)r * THREADS + tid < c) s[atomicAdd(&ctr[min(f(key[r]), S - 1)], 1u)] = key[r];
+            if ((uint32_t)r * THREADS + tid < c) s[atomicAdd(&ctr[f(key[r])], 1u)] = key[r];
         }
         refill();
         __syncthreads();

@@ -82,7 +82,6 @@ struct LeafItem {
     uint64_t dst;        // index of the first key in the caller's output
     uint32_t count;
     uint32_t pad_;
-    K lo, hi;            // bounds of the keys when the splitters give them (lo > hi: not known)
 };
 
 // Leaf size classes.  Class 0 is one warp per bucket (a 256-key bitonic
@@ -913,30 +912,15 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
     constexpr int LIST_NEXT = NCLASS + 1;  // lists 0..NCLASS-1 leaves, NCLASS copies, NCLASS+1 next level
     __shared__ uint32_t list_n[NCLASS + 2], list_base[NCLASS + 2];
     __shared__ uint32_t st_max, st_nonempty;
-    __shared__ K bnd_lo[NB], bnd_hi[NB];  // bounds of range bucket b between two splitters
     __shared__ unsigned long long st_keys, st_next_keys;
     __shared__ double st_sq;
     if (b < NCLASS + 2) list_n[b] = 0;
-    bnd_lo[b] = KeyMax<K>::value;
-    bnd_hi[b] = K(0);
     if (b == 0) {
         st_max = 0;
         st_nonempty = 0;
         st_keys = 0;
         st_next_keys = 0;
         st_sq = 0.0;
-    }
-    __syncthreads();
-    if (!use_learned) {
-        // range bucket of splitter t holds keys in (uniq[t-1], uniq[t]] (the
-        // first and the last range bucket are open at one end)
-        const SplitSet<K>& ss = a.splits[s];
-        const uint32_t t = (uint32_t)b;
-        if (t > 0 && t < ss.nuniq) {
-            const uint32_t rb = ss.range_b[t];
-            bnd_lo[rb] = ss.uniq[t - 1];
-            bnd_hi[rb] = ss.uniq[t];
-        }
     }
     __syncthreads();
     const bool is_eq = (bucket_eq[b >> 5] >> (b & 31)) & 1u;
@@ -1003,8 +987,6 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
                 it.dst = dst + o;
                 it.count = (uint32_t)((c - o) < COPY_CHUNK ? (c - o) : COPY_CHUNK);
                 it.pad_ = 0;
-                it.lo = KeyMax<K>::value;
-                it.hi = K(0);
                 a.items[CLS_COPY][slot] = it;
             } else {
                 raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
@@ -1017,8 +999,6 @@ __global__ void __launch_bounds__(NB) plan_kernel(PlanArgs<K> a, uint32_t nsegs)
             it.dst = dst;
             it.count = (uint32_t)c;
             it.pad_ = 0;
-            it.lo = bnd_lo[b];
-            it.hi = bnd_hi[b];
             a.items[list][first] = it;
         } else {
             raise_error(&a.ctl->err, DEV_ERR_CAPACITY);
@@ -1149,7 +1129,7 @@ __global__ void __launch_bounds__(THREADS, leaf_min_blocks(THREADS))
         const size_t dst = cur.dst;
         block_slot_sort<K, THREADS, EPT, false>(
             key, cur.count, [&](uint32_t i, K x) { out.store(dst + i, x); }, [&]() { load(next); },
-            [&]() { uneven[atomicAdd(n_uneven, 1u)] = cur; }, smem_raw, red, cur.lo, cur.hi);
+            [&]() { uneven[atomicAdd(n_uneven, 1u)] = cur; }, smem_raw, red);
         cur = next;
     }
 }
